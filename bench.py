@@ -1,0 +1,317 @@
+"""Benchmark: cell-steps/s of the FP64 engine on her_model_2014.
+
+Workload (the batched configuration): 4096 parameter sets, each template
+parameter scaled by exp(U(ln 0.5, ln 2)) per set (seeded), 200 cells per set
+on DENSE's default hexagonal tissue (-c 200 -w 4), dt 0.01 min, 1200 min,
+Oscillation of mh1 over every cell sampled every 0.1 min (4-minute window).
+A cell-step is one forward-Euler step of one cell of one set.
+
+A timed step is one launch of the step kernel that advances every set by
+1200/K minutes (K = --steps), so K steps cover the whole horizon; W warm-up
+launches run first on the same batch, which is then reset (outside the
+timed region).  The batch's history rings and oscillation windows total
+well over the 126 MB L2, so no flush is needed between steps.
+
+e2e: the same metric through the public API with host buffers: building the
+batch from host arrays (host->device copies), the full horizon, and reading
+every set's oscillation amplitude/period back to the host.
+
+Multi-GPU (torchrun): each rank runs its own batch (sets shard with no
+exchange; scaling is weak); times are the max over ranks.
+
+--impl reference: DENSE's own deterministic path (compiled from its sources
+into oracle/_ref by oracle/build.py) on every host core, each step a bounded
+sample of the same workload.
+"""
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic cost of one her_model_2014 cell-step (FP64):
+#  bytes: the lag-0 state read (14 x 8) and written (14 x 8) plus the
+#         distinct delayed reads (pd, ph11 x3, ph713 x3, md, mh13 and the
+#         neighbour-averaged pd row: 10 x 8) = 304 B;
+#  flops: 34 rates (~89 mul/add/div incl. the two neighbour averages), 52
+#         delta terms (mul + add) and 14 Euler updates (mul + add) = 221.
+BYTES_PER_CELL_STEP = 304
+FLOPS_PER_CELL_STEP = 221
+
+METRIC = "cell-steps/s (FP64 plain)"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, gpu):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(num_sets, minutes, seed):
+    from dense_b200 import workloads
+    sets = workloads.log_uniform_sets(num_sets, cells=200, width=4, duration=minutes, seed=seed)
+    return sets, workloads.batch_analyses(200, 0.1)
+
+
+def cpu_sample(kind_pref="reference", num_sets=2, minutes=300.0, seed=7):
+    """DENSE (or the oracle port) on the host, one core, a bounded sample:
+    `num_sets` sets of the workload for `minutes` simulated minutes."""
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    from oracle.pyoracle import load_oracle, load_ref
+    lib = load_ref("her_model_2014") if kind_pref == "reference" else None
+    kind = "reference"
+    if lib is None:
+        lib, kind = load_oracle("her_model_2014"), "port"
+    P = workloads.log_uniform_params(num_sets, seed=seed)
+    off, ids = default_graph(200, 4)
+    mh1 = workloads.her_species("mh1")
+    steps = 0
+    t0 = time.perf_counter()
+    for i in range(num_sets):
+        sim = lib.create(off, ids, np.tile(P[i], (200, 1)), P[i], None, 0.01)
+        sim.add_oscillation(mh1, 0, 200, 0.0, float("inf"), 4.0, 0.1)
+        chunks = sim.run(minutes, 0.1)
+        steps += chunks * int(0.1 / 0.01) * 200
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "unit": "cell-steps/s", "cores": 1, "kind": kind,
+            "sample": "%d sets x 200 cells x %g min (dt 0.01, Oscillation mh1 every 0.1 min) of the workload, "
+                      "one host core, %.1f s" % (num_sets, minutes, dt)}
+
+
+def _ref_worker(args):
+    seed, minutes = args
+    r = cpu_sample("reference", num_sets=1, minutes=minutes, seed=seed)
+    return r["value"], r["kind"]
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0))
+    ctx = mp.get_context("spawn")
+    minutes = 60.0
+    with ctx.Pool(cores) as pool:
+        for w in range(a.warmup):
+            pool.map(_ref_worker, [(100 + w * cores + i, 10.0) for i in range(cores)])
+        vals, kinds = [], set()
+        t0 = time.perf_counter()
+        for k in range(a.steps):
+            out = pool.map(_ref_worker, [(1000 + k * cores + i, minutes) for i in range(cores)])
+            kinds.update(x[1] for x in out)
+        elapsed = time.perf_counter() - t0
+    cell_steps = a.steps * cores * 200 * int(round(minutes / 0.1)) * 10
+    value = cell_steps / elapsed
+    kind = "reference" if kinds == {"reference"} else "port"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed / a.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "her_model_2014 log-uniform [0.5,2]x sets, 200 cells (-c 200 -w 4), dt 0.01, "
+                                   "Oscillation(mh1) every 0.1 min", "sample_per_step": "%d sets x %g min, one set "
+                                   "per core" % (cores, minutes)},
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind,
+                             "sample": "%d host processes, each DENSE on one set of 200 cells for %g min per step"
+                                       % (cores, minutes)},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--sets", type=int, default=4096)
+    ap.add_argument("--minutes", type=float, default=1200.0)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    if a.impl == "reference":
+        return run_reference(a)
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from dense_b200 import engine as E
+
+    precision = E.FP64 if a.precision == "fp64" else E.FP32_KAHAN
+    sets, analyses = build_workload(a.sets, a.minutes, seed=2 + rank)
+    batch = E.Batch("her_model_2014", sets, 0.01, 0.1, analyses, precision=precision, device=local)
+    info = batch.info()
+    total_chunks = int(math.ceil(a.minutes / 0.1))
+    per_step = int(math.ceil(total_chunks / a.steps))
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(a.warmup):
+        batch.run(per_step, stream=sptr, graph=True)
+    barrier()
+    batch.reset(stream=sptr)
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    clocks = Clocks(local)
+    barrier()
+    ev[0].record(stream)
+    for k in range(a.steps):
+        batch.run(per_step, stream=sptr, graph=True)
+        ev[k + 1].record(stream)
+    stream.synchronize()
+    barrier()
+    clk = clocks.stop()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(a.steps)]
+    total_ms = ev[0].elapsed_time(ev[a.steps])
+    chunks, _ = batch.progress()
+    status = batch.status()
+    done_cell_steps = int(sum(int(chunks[i]) * 10 * sets[i].num_cells for i in range(len(sets))))
+    t = torch.tensor([total_ms, done_cell_steps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        tm = t.clone()
+        torch.distributed.all_reduce(tm[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(tm[1:], op=torch.distributed.ReduceOp.SUM)
+        t = tm
+    total_ms_max, all_cell_steps = float(t[0]), float(t[1])
+    value = all_cell_steps / (total_ms_max / 1e3)
+    per_launch_cell_steps = done_cell_steps / a.steps
+    avg_launch_s = (total_ms / a.steps) / 1e3
+
+    # ---- e2e through the public API, host buffers
+    e2e_times = []
+    h2d = d2h = 0
+    for k in range(a.e2e_steps):
+        barrier()
+        t0 = time.perf_counter()
+        b = E.Batch("her_model_2014", sets, 0.01, 0.1, analyses, precision=precision, device=local)
+        b.run(-1)
+        res = [b.oscillation(0, i) for i in range(len(sets))]
+        b.close()
+        barrier()
+        e2e_times.append(time.perf_counter() - t0)
+        if k == 0:
+            h2d = sum(s.num_cells * len(s.set_params) * 8 + s.nbr_offsets.nbytes + s.nbr_ids.nbytes for s in sets)
+            d2h = sum(r["amps"].nbytes + r["pers"].nbytes + r["avg_peak"].nbytes + r["ncrit"].nbytes for r in res)
+    e2e_s = max(e2e_times)
+    if world > 1:
+        x = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(x[0])
+    e2e_value = world * info["total_cell_steps"] / e2e_s
+
+    hbm, peak_src = peaks()
+    achieved_gbs = BYTES_PER_CELL_STEP * per_launch_cell_steps / avg_launch_s / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            d = json.load(f)
+        traffic = d.get("bytes_per_cell_step", None)
+        if traffic is not None:
+            traffic = traffic * per_launch_cell_steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = cpu_sample()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": total_ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if precision == E.FP64 else "f32+kahan", "data": "synthetic",
+            "config": {"workload": "her_model_2014: %d parameter sets (template x exp(U(ln .5, ln 2)) per set), "
+                                   "200 cells each (-c 200 -w 4), dt 0.01 min, %g min, Oscillation(mh1, all "
+                                   "cells, window 4 min) every 0.1 min" % (a.sets, a.minutes),
+                       "sets_per_gpu": a.sets, "step": "one launch advancing every set %d chunks (%g min)"
+                       % (per_step, per_step * 0.1), "l2": "inputs larger than L2 (history rings + "
+                       "windows %.0f MB per GPU)" % (info["device_bytes"] / 1e6),
+                       "parallelism": "sets sharded across %d GPU(s), no exchange" % world},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm, "traffic": traffic,
+                         "basis": "%d algorithmic bytes per cell-step (state read+write, delayed reads); peak "
+                                  "%s (MEASURED_PEAKS.json hbm_gbs)" % (BYTES_PER_CELL_STEP, peak_src),
+                         "fp64_flops_per_s": FLOPS_PER_CELL_STEP * per_launch_cell_steps / avg_launch_s},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": a.e2e_steps,
+                    "what": "Batch() from host arrays + full horizon + per-set oscillation results to host"},
+            "gpu_launches": a.steps,
+            "clocks": clk,
+            "step_ms": {"min": min(step_ms), "max": max(step_ms)},
+            "status_nonzero_sets": int((status != 0).sum()),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

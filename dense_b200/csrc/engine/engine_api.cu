@@ -1,0 +1,612 @@
+// Host side of the engine: batch set-up and the C ABI of include/dense_b200.h.
+//
+// Set-up restates, per parameter set, what DENSE's constructors compute:
+//   * max_delays per species from the delay reactions that read it
+//     (Simulation::calc_max_delays, sim/base.cpp:55-140), traced through the
+//     model's own active_rate specialisations;
+//   * DENSE's ring size S_sp = (int)(max_delays_sp / dt + 2)
+//     (baby_cl.cpp:5-15);
+//   * the lags each cell actually reads (the model's active_rate evaluated
+//     per cell with a recording context), from which the staged history
+//     depth D_sp follows;
+//   * the chunk count of run_simulation (chunks a = 0, 1, ... while
+//     a < duration / interval) and the steps per chunk (int)(interval / dt)
+//     (run_simulation.hpp:127-130, determ.cpp:11).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dense_model_api.hpp"
+#include "reaction_deltas.hpp"
+#include "model_impl.hpp"
+
+#include "dense_b200.h"
+#include "engine_launch.hpp"
+#include "engine_types.hpp"
+
+using namespace dense_b200;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (expr);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return fail(DENSE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Dependency tracer (the DummyContext of sim/base.cpp:62-95).
+struct DepContext {
+  bool* deps;
+  double getCon(specie_id sp, int = 0) const { deps[sp] = true; return 0.0; }
+  double calculateNeighborAvg(specie_id sp, int = 0) const { deps[sp] = true; return 0.0; }
+  double getRate(reaction_id) const { return 0.0; }
+  double getDelay(delay_reaction_id) const { return 0.0; }
+  double getCritVal(critspecie_id) const { return 0.0; }
+};
+
+// Records, for one cell, the lag of every history read its reactions make,
+// using the same lag arithmetic as the device context.  Concentrations are
+// stand-ins; several passes with different stand-ins reach reads behind
+// data-dependent branches.  A read missed here is still caught on the
+// device (DENSE_SET_UNSTAGED_LAG).
+struct LagTracer {
+  const double* prm;
+  const double* conc;
+  double nbr_value;
+  const int* S;
+  int* own_max;   // [NS] deepest own lag
+  int* nbr_max;   // [NS] deepest neighbour lag, -1 none
+  bool* ordered;  // a neighbour read of lag S-1
+  bool* bad;
+  double getCon(specie_id sp) const { return conc[sp]; }
+  double getCon(specie_id sp, int k) const {
+    const int s = S[sp];
+    if (k < 0 || k > s + 1) *bad = true;
+    const int lag = (((k - 1) % s) + s) % s;
+    own_max[sp] = std::max(own_max[sp], lag);
+    return conc[sp];
+  }
+  double calculateNeighborAvg(specie_id sp, int k = 0) const {
+    const int s = S[sp];
+    if (k < 0 || k > s) *bad = true;
+    const int lag = ((k % s) + s) % s;
+    if (lag == s - 1 && s > 1) *ordered = true;
+    nbr_max[sp] = std::max(nbr_max[sp], lag);
+    return nbr_value;
+  }
+  double getRate(reaction_id r) const { return prm[r]; }
+  double getDelay(delay_reaction_id d) const { return prm[NUM_REACTIONS + d]; }
+  double getCritVal(critspecie_id c) const { return prm[NUM_REACTIONS + NUM_DELAY_REACTIONS + c]; }
+};
+
+struct SetPlan {
+  SetDesc d;
+  int status = 0;
+};
+
+struct DeviceBuffer {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DeviceBuffer() {
+    if (p) cudaFree(p);
+  }
+  int alloc(size_t n) {
+    bytes = n;
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(DENSE_ERR_MEMORY, std::string("cudaMalloc(") + std::to_string(n) + "): " + cudaGetErrorString(e));
+    }
+    return DENSE_OK;
+  }
+};
+
+}  // namespace
+
+struct dense_engine {
+  int device = 0;
+  int precision = DENSE_FP64;
+  int num_sets = 0;
+  cudaStream_t stream = nullptr;
+  StepArgs args{};
+  size_t smem = 0;
+  int64_t total_cell_steps = 0;
+  int64_t device_bytes = 0;
+  std::vector<SetDesc> sets;
+  std::vector<AnalysisDesc> analyses;
+  std::vector<int> init_status;
+  DeviceBuffer d_sets, d_prog, d_params, d_nbr_off, d_nbr_idx, d_state, d_ring, d_anl, d_init_conc,
+      d_init_status;
+  std::map<int, cudaGraphExec_t> graphs;
+  ~dense_engine() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// ring sizes and traced depths for one set
+int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<double>& cell_params) {
+  const int n = in.num_cells;
+  SetDesc& d = plan.d;
+  d.n_cells = n;
+  // max_delays (base.cpp:55-140); the gradient loop there never runs
+  // (circumference_ is 0 at that point), so max_gradient is 1.
+  bool deps[NUM_REACTIONS][NUM_SPECIES] = {};
+#define REACTION(name) { DepContext c{deps[name]}; reaction<name>::active_rate(c); }
+#include "reactions_list.hpp"
+#undef REACTION
+  double max_delays[NUM_SPECIES] = {};
+  for (int dr = 0; dr < NUM_DELAY_REACTIONS; ++dr) {
+    const int r = dense_delay_reaction_of[dr];
+    const double pert = in.perturb ? in.perturb[r] : 0.0;
+    for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+      if (!deps[r][sp]) continue;
+      const double v = in.set_params[NUM_REACTIONS + dr] * 1.0 * (1.0 + pert);
+      max_delays[sp] = (v < max_delays[sp]) ? max_delays[sp] : v;
+    }
+  }
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+    const double v = max_delays[sp] / dt + 2;  // baby_cl.cpp:10
+    if (!(v >= 1.0 && v < 2147483647.0))
+      return fail(DENSE_ERR_INVALID, "ring size of species " + std::to_string(sp) + " is not a positive int");
+    d.S[sp] = static_cast<int>(v);
+  }
+  // per-cell parameters, [NP][n] for the device; NaN rates/delays reject
+  // the set, as DENSE's getRate/getDelay throw (sim/base.hpp:398-412)
+  cell_params.resize(static_cast<size_t>(NUM_PARAMS) * n);
+  for (int c = 0; c < n; ++c) {
+    const double* p = in.cell_params ? in.cell_params + static_cast<size_t>(c) * NUM_PARAMS : in.set_params;
+    for (int i = 0; i < NUM_PARAMS; ++i) {
+      cell_params[static_cast<size_t>(i) * n + c] = p[i];
+      if (i < NUM_REACTIONS + NUM_DELAY_REACTIONS && std::isnan(p[i])) plan.status |= kSetNanParam;
+    }
+  }
+  // traced lags
+  int own_max[NUM_SPECIES], nbr_max[NUM_SPECIES];
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) { own_max[sp] = 0; nbr_max[sp] = -1; }
+  bool ordered = false, bad = false;
+  double prm[NUM_PARAMS];
+  double conc[NUM_SPECIES];
+  const double nbr_values[4] = {0.0, 2.0, 0.5, 7.25};
+  // cells sharing the set's parameters all read the same lags: trace one
+  const int traced = in.cell_params ? n : 1;
+  for (int c = 0; c < traced; ++c) {
+    for (int i = 0; i < NUM_PARAMS; ++i) prm[i] = cell_params[static_cast<size_t>(i) * n + c];
+    for (int pass = 0; pass < 4; ++pass) {
+      for (int sp = 0; sp < NUM_SPECIES; ++sp) conc[sp] = pass == 0 ? 0.0 : (pass == 1 ? 1.0 : 0.37 * (sp + pass));
+      LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad};
+#define REACTION(name) reaction<name>::active_rate(t);
+#include "reactions_list.hpp"
+#undef REACTION
+    }
+  }
+  if (ordered) plan.status |= kSetOrderedReads;
+  if (bad) plan.status |= kSetBadDelay;
+  int64_t off = 0;
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+    int depth = 0;
+    if (own_max[sp] >= 1) depth = own_max[sp] + 1;
+    if (nbr_max[sp] >= 0) depth = std::max(depth, nbr_max[sp] + 2);
+    depth = std::min(depth, d.S[sp] + 1);
+    d.D[sp] = depth;
+    d.ring_off[sp] = off;
+    off += static_cast<int64_t>(depth) * n;
+  }
+  // chunk count: a = 0, 1, ... while a < duration / interval
+  return DENSE_OK;
+}
+
+int64_t ring_elems(const SetDesc& d) {
+  int64_t t = 0;
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) t += static_cast<int64_t>(d.D[sp]) * d.n_cells;
+  return t;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dense_model_get_info(dense_model_info* out) {
+  if (!out) return fail(DENSE_ERR_INVALID, "null out");
+  out->num_species = NUM_SPECIES;
+  out->num_reactions = NUM_REACTIONS;
+  out->num_delay_reactions = NUM_DELAY_REACTIONS;
+  out->num_critical_species = NUM_CRITICAL_SPECIES;
+  out->num_params = NUM_PARAMS;
+  return DENSE_OK;
+}
+
+const char* dense_model_specie_name(int i) { return (i >= 0 && i < NUM_SPECIES) ? dense_specie_names[i] : nullptr; }
+const char* dense_model_reaction_name(int i) { return (i >= 0 && i < NUM_REACTIONS) ? dense_reaction_names[i] : nullptr; }
+const char* dense_last_error(void) { return g_error.c_str(); }
+
+int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set_desc* in_sets,
+                        dense_engine** out) {
+  if (!run || !out || num_sets <= 0 || !in_sets) return fail(DENSE_ERR_INVALID, "null argument or no sets");
+  *out = nullptr;
+  if (!(run->step_size > 0.0) || !(run->analysis_interval > 0.0))
+    return fail(DENSE_ERR_INVALID, "step size and analysis interval must be positive");
+  if (run->precision != DENSE_FP64 && run->precision != DENSE_FP32_KAHAN)
+    return fail(DENSE_ERR_INVALID, "unknown precision");
+  if (run->num_analyses < 0 || run->num_analyses > kMaxAnalyses)
+    return fail(DENSE_ERR_UNSUPPORTED, "at most " + std::to_string(kMaxAnalyses) + " analyses per batch");
+  const double dt = run->step_size, interval = run->analysis_interval;
+  const double steps_d = interval / dt;  // determ.cpp:11
+  if (!(steps_d < 2147483647.0)) return fail(DENSE_ERR_INVALID, "interval / step size too large");
+  const int steps_per_chunk = static_cast<int>(steps_d);
+
+  std::unique_ptr<dense_engine> e(new dense_engine());
+  e->device = run->device;
+  e->precision = run->precision;
+  e->num_sets = num_sets;
+  CUDA_TRY(cudaSetDevice(run->device));
+
+  // ---- analyses
+  int min_cells = kMaxCellsPerSet + 1;
+  for (int s = 0; s < num_sets; ++s) min_cells = std::min(min_cells, in_sets[s].num_cells);
+  int64_t anl_block = 0;
+  for (int ai = 0; ai < run->num_analyses; ++ai) {
+    const dense_analysis_desc& in = run->analyses[ai];
+    AnalysisDesc A{};
+    A.kind = in.kind;
+    A.cmin = in.cell_start;
+    A.cmax = in.cell_end;
+    A.t0 = in.time_start;
+    A.t1 = in.time_end;
+    if (A.cmin < 0 || A.cmax < A.cmin || A.cmax > min_cells)
+      return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": cell range outside the tissue");
+    if (in.kind == DENSE_ANALYSIS_CONCCHECK && in.num_species == 0) {
+      A.nsp = NUM_SPECIES;
+      for (int i = 0; i < NUM_SPECIES; ++i) A.sp[i] = i;
+    } else {
+      if (in.num_species <= 0 || in.num_species > NUM_SPECIES || !in.species)
+        return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": bad species list");
+      A.nsp = in.num_species;
+      for (int i = 0; i < in.num_species; ++i) {
+        if (in.species[i] < 0 || in.species[i] >= NUM_SPECIES)
+          return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": bad species id");
+        A.sp[i] = in.species[i];
+      }
+    }
+    const int64_t m = A.cmax - A.cmin;
+    A.off = anl_block;
+    if (in.kind == DENSE_ANALYSIS_BASIC) {
+      anl_block += 3 * A.nsp + 2 + 3 * m * A.nsp;
+    } else if (in.kind == DENSE_ANALYSIS_OSCILLATION) {
+      if (!(in.anlys_intvl > 0.0) || !(in.win_range >= 0.0))
+        return fail(DENSE_ERR_INVALID, "oscillation: bad window");
+      const double rs = in.win_range / in.anlys_intvl;  // oscillation.hpp:64
+      if (!(rs < 1e6)) return fail(DENSE_ERR_UNSUPPORTED, "oscillation window too long");
+      A.range_steps = static_cast<int>(rs);
+      A.interval = in.anlys_intvl;
+      anl_block += 2 + m * A.nsp * kOscCellDoubles + static_cast<int64_t>(A.nsp) * (A.range_steps + 1) * m;
+    } else if (in.kind == DENSE_ANALYSIS_CONCCHECK) {
+      A.lo = in.lower;
+      A.hi = in.upper;
+      anl_block += 1;
+    } else {
+      return fail(DENSE_ERR_INVALID, "unknown analysis kind");
+    }
+    anl_block = (anl_block + 1) & ~int64_t(1);
+    e->analyses.push_back(A);
+  }
+
+  // ---- sets
+  std::vector<double> params_all, conc_all(static_cast<size_t>(num_sets) * NUM_SPECIES, 0.0);
+  std::vector<int> off_all, idx_all;
+  int64_t cells_total = 0, ring_total = 0;
+  int max_cells = 0;
+  e->sets.resize(num_sets);
+  e->init_status.resize(num_sets);
+  std::vector<double> cp;
+  for (int s = 0; s < num_sets; ++s) {
+    const dense_set_desc& in = in_sets[s];
+    const std::string where = "set " + std::to_string(s) + ": ";
+    if (in.num_cells <= 0 || in.num_cells > 256)
+      return fail(DENSE_ERR_UNSUPPORTED, where + "1..256 cells per set are supported");
+    if (!in.nbr_offsets || !in.nbr_ids || !in.set_params) return fail(DENSE_ERR_INVALID, where + "null input");
+    if (!(in.duration >= 0.0)) return fail(DENSE_ERR_INVALID, where + "negative duration");
+    const int n = in.num_cells;
+    if (in.nbr_offsets[0] != 0) return fail(DENSE_ERR_INVALID, where + "CSR offsets must start at 0");
+    for (int c = 0; c < n; ++c) {
+      if (in.nbr_offsets[c + 1] < in.nbr_offsets[c]) return fail(DENSE_ERR_INVALID, where + "CSR offsets decrease");
+      for (int k = in.nbr_offsets[c]; k < in.nbr_offsets[c + 1]; ++k) {
+        const int v = in.nbr_ids[k];
+        if (v < 0 || v >= n) return fail(DENSE_ERR_INVALID, where + "neighbour id outside the tissue");
+        if (k > in.nbr_offsets[c] && in.nbr_ids[k - 1] >= v)
+          return fail(DENSE_ERR_INVALID, where + "neighbour ids must ascend (DENSE keeps them in a std::set)");
+      }
+    }
+    SetPlan plan;
+    int rc = plan_set(in, dt, plan, cp);
+    if (rc != DENSE_OK) return fail(rc, where + g_error);
+    SetDesc& d = plan.d;
+    const double chunks = in.duration / interval;  // run_simulation.hpp:127
+    if (!(chunks < 2147483647.0)) return fail(DENSE_ERR_INVALID, where + "too many chunks");
+    d.n_chunks = static_cast<int>(std::ceil(chunks));
+    d.steps_per_chunk = steps_per_chunk;
+    d.cell_base = cells_total;
+    d.nbr_base = static_cast<int64_t>(off_all.size());
+    d.ring_base = ring_total;
+    d.anl_base = anl_block * s;
+    const int e0 = static_cast<int>(idx_all.size());
+    for (int c = 0; c <= n; ++c) off_all.push_back(e0 + in.nbr_offsets[c]);
+    idx_all.insert(idx_all.end(), in.nbr_ids, in.nbr_ids + in.nbr_offsets[n]);
+    params_all.insert(params_all.end(), cp.begin(), cp.end());
+    if (in.init_conc)
+      for (int sp = 0; sp < NUM_SPECIES; ++sp) conc_all[static_cast<size_t>(s) * NUM_SPECIES + sp] = in.init_conc[sp];
+    // a set whose reads alias rows written in the same step (Gauss-Seidel
+    // order, e.g. neighbour averages with delay 1 and no delay reactions)
+    // is not run by this schedule
+    e->init_status[s] = plan.status;
+    cells_total += n;
+    ring_total += ring_elems(d);
+    ring_total = (ring_total + 31) & ~int64_t(31);
+    max_cells = std::max(max_cells, n);
+    e->total_cell_steps += static_cast<int64_t>(n) * d.n_chunks * steps_per_chunk;
+    e->sets[s] = d;
+  }
+
+  // ---- device buffers
+  CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  const size_t tsz = run->precision == DENSE_FP64 ? sizeof(double) : sizeof(float);
+  int rc;
+  if ((rc = e->d_sets.alloc(sizeof(SetDesc) * num_sets))) return rc;
+  if ((rc = e->d_prog.alloc(sizeof(SetProgress) * num_sets))) return rc;
+  if ((rc = e->d_params.alloc(sizeof(double) * params_all.size()))) return rc;
+  if ((rc = e->d_nbr_off.alloc(sizeof(int) * off_all.size()))) return rc;
+  if ((rc = e->d_nbr_idx.alloc(sizeof(int) * idx_all.size()))) return rc;
+  if ((rc = e->d_state.alloc(tsz * 2 * NUM_SPECIES * cells_total))) return rc;
+  if ((rc = e->d_ring.alloc(tsz * ring_total))) return rc;
+  if ((rc = e->d_anl.alloc(sizeof(double) * anl_block * num_sets))) return rc;
+  if ((rc = e->d_init_conc.alloc(sizeof(double) * conc_all.size()))) return rc;
+  if ((rc = e->d_init_status.alloc(sizeof(int) * num_sets))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(e->d_sets.p, e->sets.data(), sizeof(SetDesc) * num_sets, cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_params.p, params_all.data(), sizeof(double) * params_all.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_nbr_off.p, off_all.data(), sizeof(int) * off_all.size(), cudaMemcpyHostToDevice, e->stream));
+  if (!idx_all.empty())
+    CUDA_TRY(cudaMemcpyAsync(e->d_nbr_idx.p, idx_all.data(), sizeof(int) * idx_all.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_init_conc.p, conc_all.data(), sizeof(double) * conc_all.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_init_status.p, e->init_status.data(), sizeof(int) * num_sets, cudaMemcpyHostToDevice, e->stream));
+  e->device_bytes = static_cast<int64_t>(e->d_sets.bytes + e->d_prog.bytes + e->d_params.bytes + e->d_nbr_off.bytes +
+                                         e->d_nbr_idx.bytes + e->d_state.bytes + e->d_ring.bytes + e->d_anl.bytes +
+                                         e->d_init_conc.bytes + e->d_init_status.bytes);
+
+  StepArgs& a = e->args;
+  a.sets = static_cast<const SetDesc*>(e->d_sets.p);
+  a.prog = static_cast<SetProgress*>(e->d_prog.p);
+  a.params = static_cast<const double*>(e->d_params.p);
+  a.nbr_off = static_cast<const int*>(e->d_nbr_off.p);
+  a.nbr_idx = static_cast<const int*>(e->d_nbr_idx.p);
+  a.state = e->d_state.p;
+  a.ring = e->d_ring.p;
+  a.anl = static_cast<double*>(e->d_anl.p);
+  for (size_t i = 0; i < e->analyses.size(); ++i) a.analyses[i] = e->analyses[i];
+  a.n_analyses = static_cast<int>(e->analyses.size());
+  a.num_sets = num_sets;
+  a.dt = dt;
+  a.interval = interval;
+  a.chunk_count = -1;
+  a.block_threads = std::max(32, (max_cells + 31) / 32 * 32);
+  e->smem = a.n_analyses > 0 ? sizeof(double) * NUM_SPECIES * a.block_threads : 0;
+
+  rc = dense_engine_reset(e.get(), nullptr);
+  if (rc != DENSE_OK) return rc;
+  *out = e.release();
+  return DENSE_OK;
+}
+
+int dense_engine_reset(dense_engine* e, void* stream) {
+  if (!e) return fail(DENSE_ERR_INVALID, "null engine");
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  const double* ic = static_cast<const double*>(e->d_init_conc.p);
+  const int* is = static_cast<const int*>(e->d_init_status.p);
+  CUDA_TRY(e->precision == DENSE_FP64 ? launch_init_fp64(e->args, ic, is, s) : launch_init_fp32(e->args, ic, is, s));
+  return DENSE_OK;
+}
+
+int dense_engine_run(dense_engine* e, int num_chunks, void* stream) {
+  if (!e) return fail(DENSE_ERR_INVALID, "null engine");
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  StepArgs a = e->args;
+  a.chunk_count = num_chunks < 0 ? -1 : num_chunks;
+  CUDA_TRY(e->precision == DENSE_FP64 ? launch_step_fp64(a, e->smem, s) : launch_step_fp32(a, e->smem, s));
+  return DENSE_OK;
+}
+
+int dense_engine_run_graph(dense_engine* e, int num_chunks, void* stream) {
+  if (!e) return fail(DENSE_ERR_INVALID, "null engine");
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  auto it = e->graphs.find(num_chunks);
+  if (it == e->graphs.end()) {
+    // first use: make sure the kernel attributes are set outside capture
+    StepArgs a0 = e->args;
+    a0.chunk_count = 0;
+    CUDA_TRY(e->precision == DENSE_FP64 ? launch_step_fp64(a0, e->smem, s) : launch_step_fp32(a0, e->smem, s));
+    cudaStream_t cap;
+    CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    StepArgs a = e->args;
+    a.chunk_count = num_chunks < 0 ? -1 : num_chunks;
+    cudaError_t le = e->precision == DENSE_FP64 ? launch_step_fp64(a, e->smem, cap) : launch_step_fp32(a, e->smem, cap);
+    cudaError_t ce = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    CUDA_TRY(le);
+    CUDA_TRY(ce);
+    cudaGraphExec_t ge;
+    cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CUDA_TRY(ie);
+    it = e->graphs.emplace(num_chunks, ge).first;
+  }
+  CUDA_TRY(cudaGraphLaunch(it->second, s));
+  return DENSE_OK;
+}
+
+int dense_engine_sync(dense_engine* e) {
+  if (!e) return fail(DENSE_ERR_INVALID, "null engine");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaDeviceSynchronize());
+  return DENSE_OK;
+}
+
+static int read_progress(dense_engine* e, std::vector<SetProgress>& p) {
+  p.resize(e->num_sets);
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(p.data(), e->d_prog.p, sizeof(SetProgress) * e->num_sets, cudaMemcpyDeviceToHost));
+  return DENSE_OK;
+}
+
+int dense_engine_status(dense_engine* e, int32_t* out) {
+  if (!e || !out) return fail(DENSE_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<SetProgress> p;
+  int rc = read_progress(e, p);
+  if (rc) return rc;
+  for (int s = 0; s < e->num_sets; ++s) out[s] = p[s].status;
+  return DENSE_OK;
+}
+
+int dense_engine_progress(dense_engine* e, int32_t* chunks, double* age) {
+  if (!e) return fail(DENSE_ERR_INVALID, "null engine");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<SetProgress> p;
+  int rc = read_progress(e, p);
+  if (rc) return rc;
+  for (int s = 0; s < e->num_sets; ++s) {
+    if (chunks) chunks[s] = p[s].chunk;
+    if (age) age[s] = p[s].age;
+  }
+  return DENSE_OK;
+}
+
+int dense_engine_read_state(dense_engine* e, int set, double* out) {
+  if (!e || !out || set < 0 || set >= e->num_sets) return fail(DENSE_ERR_INVALID, "bad argument");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  const SetDesc& d = e->sets[set];
+  const size_t cnt = static_cast<size_t>(NUM_SPECIES) * d.n_cells;
+  if (e->precision == DENSE_FP64) {
+    CUDA_TRY(cudaMemcpy(out, static_cast<double*>(e->d_state.p) + d.cell_base * 2 * NUM_SPECIES,
+                        sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> tmp(cnt);
+    CUDA_TRY(cudaMemcpy(tmp.data(), static_cast<float*>(e->d_state.p) + d.cell_base * 2 * NUM_SPECIES,
+                        sizeof(float) * cnt, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < cnt; ++i) out[i] = tmp[i];
+  }
+  return DENSE_OK;
+}
+
+static int read_analysis_block(dense_engine* e, int analysis, int set, int kind, std::vector<double>& blk,
+                               const AnalysisDesc** A) {
+  if (!e || set < 0 || set >= e->num_sets || analysis < 0 || analysis >= static_cast<int>(e->analyses.size()))
+    return fail(DENSE_ERR_INVALID, "bad analysis or set index");
+  *A = &e->analyses[analysis];
+  if ((*A)->kind != kind) return fail(DENSE_ERR_INVALID, "analysis kind mismatch");
+  const SetDesc& d = e->sets[set];
+  int64_t len;
+  const int64_t m = (*A)->cmax - (*A)->cmin, nsp = (*A)->nsp;
+  if (kind == kBasic) len = 3 * nsp + 2 + 3 * m * nsp;
+  else len = 2 + m * nsp * kOscCellDoubles;
+  blk.resize(len);
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(blk.data(), static_cast<double*>(e->d_anl.p) + d.anl_base + (*A)->off, sizeof(double) * len,
+                      cudaMemcpyDeviceToHost));
+  return DENSE_OK;
+}
+
+int dense_engine_read_basic(dense_engine* e, int analysis, int set, double* mins, double* sums, double* maxs,
+                            double* cell_mins, double* cell_sums, double* cell_maxs, int* samples, double* time) {
+  std::vector<double> b;
+  const AnalysisDesc* A;
+  int rc = read_analysis_block(e, analysis, set, kBasic, b, &A);
+  if (rc) return rc;
+  const int n = A->nsp;
+  const size_t mn = static_cast<size_t>(A->cmax - A->cmin) * n;
+  for (int i = 0; i < n; ++i) {
+    if (mins) mins[i] = b[i];
+    if (maxs) maxs[i] = b[n + i];
+    if (sums) sums[i] = b[2 * n + i];
+  }
+  if (samples) *samples = static_cast<int>(b[3 * n]);
+  if (time) *time = b[3 * n + 1];
+  const double* cb = b.data() + 3 * n + 2;
+  for (size_t k = 0; k < mn; ++k) {
+    if (cell_mins) cell_mins[k] = cb[k];
+    if (cell_maxs) cell_maxs[k] = cb[mn + k];
+    if (cell_sums) cell_sums[k] = cb[2 * mn + k];
+  }
+  return DENSE_OK;
+}
+
+int dense_engine_read_oscillation(dense_engine* e, int analysis, int set, double* amps, double* periods,
+                                  double* avg_peaks, int* num_crit, int* samples, double* time) {
+  std::vector<double> b;
+  const AnalysisDesc* A;
+  int rc = read_analysis_block(e, analysis, set, kOscillation, b, &A);
+  if (rc) return rc;
+  const size_t k = static_cast<size_t>(A->cmax - A->cmin) * A->nsp;
+  const OscCell* cells = reinterpret_cast<const OscCell*>(b.data() + 2);
+  for (size_t i = 0; i < k; ++i) {
+    if (amps) amps[i] = cells[i].amp;
+    if (periods) periods[i] = cells[i].per;
+    if (avg_peaks) avg_peaks[i] = cells[i].avg_peak;
+    if (num_crit) num_crit[i] = static_cast<int>(cells[i].ncrit);
+  }
+  if (samples) *samples = static_cast<int>(b[0]);
+  if (time) *time = b[1];
+  return DENSE_OK;
+}
+
+int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int64_t* device_bytes, int* max_block_threads) {
+  if (!e) return fail(DENSE_ERR_INVALID, "null engine");
+  if (total_cell_steps) *total_cell_steps = e->total_cell_steps;
+  if (device_bytes) *device_bytes = e->device_bytes;
+  if (max_block_threads) *max_block_threads = e->args.block_threads;
+  return DENSE_OK;
+}
+
+int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D) {
+  if (!e || set < 0 || set >= e->num_sets) return fail(DENSE_ERR_INVALID, "bad argument");
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+    if (S) S[sp] = e->sets[set].S[sp];
+    if (D) D[sp] = e->sets[set].D[sp];
+  }
+  return DENSE_OK;
+}
+
+int dense_engine_destroy(dense_engine* e) {
+  if (!e) return DENSE_OK;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  delete e;
+  return DENSE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,16 @@
+// Kernel launchers of the per-precision translation units.
+#ifndef DENSE_B200_ENGINE_LAUNCH_HPP
+#define DENSE_B200_ENGINE_LAUNCH_HPP
+
+#include <cuda_runtime.h>
+
+#include "engine_types.hpp"
+
+namespace dense_b200 {
+cudaError_t launch_init_fp64(const StepArgs& a, const double* init_conc, const int* init_status, cudaStream_t s);
+cudaError_t launch_step_fp64(const StepArgs& a, size_t smem, cudaStream_t s);
+cudaError_t launch_init_fp32(const StepArgs& a, const double* init_conc, const int* init_status, cudaStream_t s);
+cudaError_t launch_step_fp32(const StepArgs& a, size_t smem, cudaStream_t s);
+}  // namespace dense_b200
+
+#endif

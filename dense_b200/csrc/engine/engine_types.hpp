@@ -1,0 +1,105 @@
+// Device-side descriptors shared by the step kernels and the host engine.
+// Compiled once per DENSE model (NUM_SPECIES etc. come from the model's
+// headers through dense_model_api.hpp).
+#ifndef DENSE_B200_ENGINE_TYPES_HPP
+#define DENSE_B200_ENGINE_TYPES_HPP
+
+#include <cstdint>
+
+#include "dense_model_api.hpp"
+
+namespace dense_b200 {
+
+constexpr int kNS = NUM_SPECIES;
+constexpr int kNR = NUM_REACTIONS;
+constexpr int kND = NUM_DELAY_REACTIONS;
+constexpr int kNP = NUM_PARAMS;
+constexpr int kMaxAnalyses = 8;
+constexpr int kMaxCellsPerSet = 1024;  // one thread per cell, one CTA per set
+
+// Per-set status bits (also the public DENSE_SET_* values).
+enum : int {
+  kSetDropped = 1,       // a concentration check rejected the set
+  kSetNanParam = 2,      // a rate or delay parameter is NaN
+  kSetUnstagedLag = 4,   // a read hit a lag the history staging did not keep
+  kSetBadDelay = 8,      // a delay DENSE would turn into an out-of-bounds read
+  kSetOrderedReads = 16, // neighbour reads of rows written in the same step
+  kSetNotRunnable = kSetNanParam | kSetOrderedReads,
+};
+
+enum AnalysisKind : int { kBasic = 1, kOscillation = 2, kConcCheck = 3 };
+
+// One analysis, identical for every set of the batch.
+struct AnalysisDesc {
+  int kind;
+  int nsp;              // observed species count (ConcCheck: 1, or NS for all)
+  int sp[kNS];          // observed species ids, in observation order
+  int cmin, cmax;       // cell range [cmin, cmax)
+  double t0, t1;        // time range [t0, t1)
+  int range_steps;      // oscillation window (range / anlys-intvl, truncated)
+  double interval;      // oscillation anlys-intvl
+  double lo, hi;        // concentration check bounds
+  int64_t off;          // offset of this analysis' state inside a set's block
+};
+
+// Layout of one analysis' per-set state (doubles unless noted), relative to
+// AnalysisDesc::off.  n = nsp, m = cmax - cmin, w = range_steps + 1.
+//  Basic:       mins[n] maxs[n] sums[n] samples time | cmins[m][n] cmaxs[m][n] csums[m][n]
+//  Oscillation: samples time | per (s, c): OscCell (as doubles) | window[s][w][m]
+//  ConcCheck:   time
+struct OscCell {
+  double start, end, current;   // queue indices (core/queue.hpp)
+  double live;                  // number of values in the window
+  double last_time, last_conc, last_peak, ncrit;
+  double t_m2, t_m1;            // times of crit points m-3 and m-2
+  double peak_sum, trough_sum, num_peaks, num_troughs, cycle_sum, cycles;
+  double amp, per, avg_peak;    // results, written by finalize
+};
+constexpr int kOscCellDoubles = sizeof(OscCell) / sizeof(double);
+
+// One parameter set of the batch.
+struct SetDesc {
+  int n_cells;
+  int n_chunks;          // analysis chunks of this set's horizon
+  int steps_per_chunk;   // (int)(interval / dt)
+  int pad0;
+  int64_t cell_base;     // first cell of this set in the per-cell arrays
+  int64_t nbr_base;      // offset of this set's CSR row offsets (n_cells + 1)
+  int64_t ring_base;     // first element of this set's history block
+  int64_t anl_base;      // first double of this set's analysis block
+  int S[kNS];            // DENSE ring size per species (baby_cl.cpp:10)
+  int D[kNS];            // staged history depth (0: lag-0 only, kept in registers)
+  int64_t ring_off[kNS]; // offset of each staged ring inside the set's block
+};
+
+// Mutable per-set progress, updated by the kernels.
+struct SetProgress {
+  int64_t step;   // Euler steps done
+  int chunk;      // chunks done
+  int status;     // kSet* bits
+  double age;     // simulated minutes (DENSE Simulation::age_)
+  int finalized;
+  int pad;
+};
+
+struct StepArgs {
+  const SetDesc* sets;
+  SetProgress* prog;
+  const double* params;     // per set: [NP][n_cells]
+  const int* nbr_off;       // per set: n_cells + 1 absolute offsets into nbr_idx
+  const int* nbr_idx;       // neighbour cell ids, local to the set, ascending
+  void* state;              // per set: [NS][n_cells] lag-0 state (T), then [NS][n_cells] Kahan terms
+  void* ring;               // history rings (T)
+  double* anl;              // analysis state
+  AnalysisDesc analyses[kMaxAnalyses];
+  int n_analyses;
+  int num_sets;
+  double dt;
+  double interval;
+  int chunk_count;          // chunks to run in this launch (-1: to the end)
+  int block_threads;
+};
+
+}  // namespace dense_b200
+
+#endif

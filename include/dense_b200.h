@@ -1,0 +1,177 @@
+/*
+ * dense_b200 -- C ABI of the B200 engine for DENSE's deterministic
+ * delay-differential simulation path.
+ *
+ * One shared library per DENSE model (libdense_b200_<model>.so): the model's
+ * specie_list.hpp, reactions_list.hpp, reaction_deltas.hpp and
+ * model_impl.hpp are compiled into it, as DENSE compiles one simulator per
+ * model (source/CMakeLists.txt:146-188).
+ *
+ * The entry points replace, for a whole batch of parameter sets at once,
+ * what DENSE does per set on the CPU:
+ *
+ *   dense_engine_create   Simulation / Deterministic_Simulation constructors
+ *                         (sim/base.cpp:35-140, sim/determ/determ.cpp:31-52,
+ *                         baby_cl.cpp:5-15) and the analysis constructors
+ *                         built by parse_analysis_entries
+ *                         (parse_analysis_entries.hpp:64-126)
+ *   dense_engine_run      run_simulation's chunk loop
+ *                         (run_simulation.hpp:127-157): analysis callbacks,
+ *                         bad-set drop, age_by -> step (determ.cpp:8-88)
+ *   dense_engine_read_*   Deterministic_Simulation::get_concentration
+ *                         (determ.hpp:73-79), BasicAnalysis and
+ *                         OscillationAnalysis results (basic.ipp:38-75,
+ *                         oscillation.ipp:6-77)
+ *   dense_engine_status   the Bad_Simulation_Error drop of run_simulation
+ *                         (run_simulation.hpp:131-150), as a per-set word
+ *
+ * Conventions: plain pointers and sizes; the caller owns host buffers, the
+ * engine owns device buffers; every function returns a DENSE_* status code
+ * (0 = OK) and no exception crosses the ABI; dense_last_error() describes
+ * the last failure of the calling thread.  Runs are stream-ordered: only
+ * dense_engine_read_* and dense_engine_sync wait for the device.
+ */
+#ifndef DENSE_B200_H
+#define DENSE_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DENSE_API __attribute__((visibility("default")))
+#else
+#define DENSE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes */
+#define DENSE_OK 0
+#define DENSE_ERR_INVALID 1     /* bad argument */
+#define DENSE_ERR_CUDA 2        /* CUDA runtime failure */
+#define DENSE_ERR_MEMORY 3      /* device allocation failed */
+#define DENSE_ERR_UNSUPPORTED 4 /* a batch the engine does not run */
+
+/* per-set status bits (dense_engine_status) */
+#define DENSE_SET_OK 0
+#define DENSE_SET_DROPPED 1        /* a concentration check rejected the set */
+#define DENSE_SET_NAN_PARAM 2      /* a rate or delay is NaN (DENSE throws) */
+#define DENSE_SET_UNSTAGED_LAG 4   /* a read needed history the staging did not keep */
+#define DENSE_SET_BAD_DELAY 8      /* a delay DENSE would read out of bounds with */
+#define DENSE_SET_ORDERED_READS 16 /* neighbour reads of rows written in the same step */
+
+/* arithmetic of a batch */
+#define DENSE_FP64 0        /* matches DENSE's CPU path bit for bit */
+#define DENSE_FP32_KAHAN 1  /* FP32 rates, Kahan-compensated FP32 state */
+
+/* analysis kinds */
+#define DENSE_ANALYSIS_BASIC 1        /* BasicAnalysis (measurement/basic.hpp) */
+#define DENSE_ANALYSIS_OSCILLATION 2  /* OscillationAnalysis (measurement/oscillation.hpp) */
+#define DENSE_ANALYSIS_CONCCHECK 3    /* ConcentrationCheck (measurement/conccheck.hpp) */
+
+typedef struct dense_model_info {
+  int num_species;
+  int num_reactions;
+  int num_delay_reactions;
+  int num_critical_species;
+  int num_params; /* rates | delays | critical values (core/parameter_set.hpp:9-13) */
+} dense_model_info;
+
+/* One parameter set (one DENSE Simulation). */
+typedef struct dense_set_desc {
+  int num_cells;              /* <= 1024 */
+  const int* nbr_offsets;     /* [num_cells + 1] CSR row offsets */
+  const int* nbr_ids;         /* neighbour cell ids, ascending per cell (std::set order) */
+  const double* set_params;   /* [num_params]: the Parameter_Set; ring sizes derive from it */
+  const double* cell_params;  /* [num_cells][num_params] per-cell parameters, or NULL:
+                                 every cell uses set_params */
+  const double* init_conc;    /* [num_species] initial value of every history row, or NULL (zeros) */
+  const double* perturb;      /* [num_reactions] -b factors entering the ring sizes, or NULL */
+  double duration;            /* simulated minutes (-t) */
+} dense_set_desc;
+
+/* One analysis, applied to every set (an <anlys> entry of analyses.xml). */
+typedef struct dense_analysis_desc {
+  int kind;                   /* DENSE_ANALYSIS_* */
+  int num_species;            /* observed species; CONCCHECK: 0 = all species */
+  const int* species;         /* [num_species] species ids */
+  int cell_start, cell_end;   /* [cell_start, cell_end) */
+  double time_start, time_end;/* [time_start, time_end) */
+  double win_range;           /* OSCILLATION: <win-range> */
+  double anlys_intvl;         /* OSCILLATION: <anlys-intvl> */
+  double lower, upper;        /* CONCCHECK bounds */
+} dense_analysis_desc;
+
+typedef struct dense_run_desc {
+  int precision;              /* DENSE_FP64 or DENSE_FP32_KAHAN */
+  double step_size;           /* dt in minutes (-s) */
+  double analysis_interval;   /* minutes between analysis samples (-u) */
+  int num_analyses;
+  const dense_analysis_desc* analyses;
+  int device;                 /* CUDA device ordinal */
+} dense_run_desc;
+
+typedef struct dense_engine dense_engine;
+
+DENSE_API int dense_model_get_info(dense_model_info* out);
+DENSE_API const char* dense_model_specie_name(int species);
+DENSE_API const char* dense_model_reaction_name(int reaction);
+DENSE_API const char* dense_last_error(void);
+
+/* Validate and stage a batch on the device (host buffers are copied). */
+DENSE_API int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set_desc* sets,
+                        dense_engine** out);
+
+/* Run the next `num_chunks` analysis chunks of every set (-1: to the end of
+   each set's horizon), on `stream` (a cudaStream_t, or NULL for the
+   engine's own stream).  Sets finishing their horizon are finalized. */
+DENSE_API int dense_engine_run(dense_engine* e, int num_chunks, void* stream);
+
+/* Same, replayed from a CUDA graph captured on first use for this chunk
+   count. */
+DENSE_API int dense_engine_run_graph(dense_engine* e, int num_chunks, void* stream);
+
+DENSE_API int dense_engine_sync(dense_engine* e);
+
+/* Reset every set to its initial state (same inputs; no reallocation). */
+DENSE_API int dense_engine_reset(dense_engine* e, void* stream);
+
+/* Per-set status words (DENSE_SET_* bits), [num_sets]. */
+DENSE_API int dense_engine_status(dense_engine* e, int32_t* out);
+
+/* Chunks done and simulated age per set, [num_sets] each. */
+DENSE_API int dense_engine_progress(dense_engine* e, int32_t* chunks, double* age);
+
+/* Lag-0 concentrations of one set, [num_species][num_cells]. */
+DENSE_API int dense_engine_read_state(dense_engine* e, int set, double* out);
+
+/* BasicAnalysis `analysis` of one set: mins/sums/maxs [n], per-cell
+   [cells][n] (any may be NULL), samples and time.  sums are the raw sums
+   DENSE keeps in `means` (basic.ipp:22-36); show() divides by
+   samples * cells. */
+DENSE_API int dense_engine_read_basic(dense_engine* e, int analysis, int set, double* mins, double* sums,
+                            double* maxs, double* cell_mins, double* cell_sums, double* cell_maxs,
+                            int* samples, double* time);
+
+/* OscillationAnalysis `analysis` of one set, [n][cells] each: average
+   amplitude, average period, mean peak ("avg peak" of show()), number of
+   critical points; plus samples and time.  Valid once the set finished. */
+DENSE_API int dense_engine_read_oscillation(dense_engine* e, int analysis, int set, double* amps,
+                                  double* periods, double* avg_peaks, int* num_crit, int* samples,
+                                  double* time);
+
+/* Batch facts: cell-steps per full run, device bytes held, history depths. */
+DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int64_t* device_bytes,
+                      int* max_block_threads);
+
+/* Staged history depth (D) and DENSE ring size (S) per species of a set. */
+DENSE_API int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D);
+
+DENSE_API int dense_engine_destroy(dense_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DENSE_B200_H */

@@ -314,7 +314,7 @@ void check_crit(Oscil& o, int s, int c) {
   double mid = q.contents[q.current];
   double hi = window_max(o.live[k]), lo = window_min(o.live[k]);
   double t = (o.samples - o.range_steps / 2) * o.interval + o.t0;
-  t = (t < 0.0) ? 0.0 : t;  // std::max<Real>(0.0, t)
+  t = (0.0 < t) ? t : 0.0;  // std::max<Real>(0.0, t)
   if (mid == hi && mid != lo) add_crit(o.crits[k], Crit{t, mid, true});
   else if (mid == lo) add_crit(o.crits[k], Crit{t, mid, false});
 }

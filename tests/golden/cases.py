@@ -1,0 +1,107 @@
+"""The small parity cases shared by the golden-fixture script and the tests.
+
+Every input is generated from a seed (numpy PCG64) and the model templates
+in dense_b200/data/templates.json, so the engine, the oracle and DENSE
+itself see identical inputs.
+"""
+
+import numpy as np
+
+from dense_b200 import workloads
+from dense_b200.tissue import default_graph
+
+INF = float("inf")
+
+
+def _her(*names):
+    return workloads.her_species(*names)
+
+
+def _set(model, cells, width, duration, cell_params=None, set_params=None, init_conc=None, perturb=None):
+    off, ids = default_graph(cells, width)
+    p = workloads.template_params(model) if set_params is None else np.asarray(set_params, np.float64)
+    cp = np.tile(p, (cells, 1)) if cell_params is None else cell_params
+    return dict(off=off, ids=ids, set_params=p, cell_params=cp, init_conc=init_conc, perturb=perturb,
+                duration=duration)
+
+
+def _her_test():
+    # DENSE's CTest "her_test" (test/her_model_2014/CMakeLists.txt:9-18,
+    # analyses.xml) minus its second Basic analysis, whose cell range
+    # (0-19) lies outside the 10-cell tissue.
+    return dict(model="her_model_2014", dt=0.01, interval=0.01,
+                sets=[_set("her_model_2014", 10, 5, 3000.0)],
+                analyses=[dict(kind="basic", species=_her("ph1", "ph7"), cells=(0, 9), t=(0.0, 15.0)),
+                          dict(kind="oscillation", species=_her("ph1", "mh1", "md"), cells=(0, 5), t=(0.0, 60.0),
+                               win=4.0, intvl=0.01)])
+
+
+def _her_pert():
+    ps = workloads.perturbed_set(cells=200, width=4, duration=60.0, seed=1)
+    nsp = len(workloads.templates()["her_model_2014"]["species"])
+    return dict(model="her_model_2014", dt=0.01, interval=0.1,
+                sets=[_set("her_model_2014", 200, 4, 60.0, cell_params=ps.cell_params)],
+                analyses=[dict(kind="basic", species=list(range(nsp)), cells=(0, 200), t=(0.0, INF)),
+                          dict(kind="oscillation", species=_her("mh1", "ph1"), cells=(0, 200), t=(0.0, INF),
+                               win=4.0, intvl=0.1)])
+
+
+def _her_sets():
+    P = workloads.log_uniform_params(6, 0.5, 2.0, seed=3)
+    return dict(model="her_model_2014", dt=0.01, interval=0.1,
+                sets=[_set("her_model_2014", 32, 4, 120.0, set_params=P[i]) for i in range(6)],
+                analyses=[dict(kind="basic", species=_her("mh1", "pd"), cells=(0, 32), t=(0.0, INF)),
+                          dict(kind="oscillation", species=_her("mh1"), cells=(0, 32), t=(0.0, INF), win=4.0,
+                               intvl=0.1)])
+
+
+def _her_delays():
+    # delays drawn from [5, 20] minutes per set, per-cell +-5% on top
+    base = workloads.template_params()
+    rng = np.random.Generator(np.random.PCG64(4))
+    sets = []
+    for i in range(4):
+        p = base.copy()
+        p[34:42] = np.where(p[34:42] > 0, rng.uniform(5.0, 20.0, 8), 0.0)
+        cp = p[None, :] * rng.uniform(0.95, 1.05, size=(16, p.size))
+        sets.append(_set("her_model_2014", 16, 4, 60.0, cell_params=cp, set_params=p))
+    return dict(model="her_model_2014", dt=0.01, interval=0.1, sets=sets,
+                analyses=[dict(kind="oscillation", species=_her("mh1", "md"), cells=(0, 16), t=(0.0, INF),
+                               win=2.0, intvl=0.1)])
+
+
+def _her_init():
+    ic = workloads.templates()["her_model_2014"]["init_conc"]
+    nsp = len(ic)
+    return dict(model="her_model_2014", dt=0.01, interval=0.05,
+                sets=[_set("her_model_2014", 20, 5, 30.0, init_conc=np.array(ic))],
+                analyses=[dict(kind="basic", species=list(range(nsp)), cells=(0, 20), t=(0.0, INF))])
+
+
+def _turing():
+    ic = workloads.templates()["turing"]["init_conc"]
+    return dict(model="turing", dt=0.01, interval=0.5,
+                sets=[_set("turing", 64, 8, 10.0, init_conc=np.array(ic))],
+                analyses=[dict(kind="basic", species=[0, 1, 2, 3], cells=(0, 64), t=(0.0, INF))])
+
+
+def _nan_test():
+    # DENSE's CTest "nan_test" (test/Nan_Test/CMakeLists.txt:6-16).
+    return dict(model="nan_test", dt=0.01, interval=0.5,
+                sets=[_set("nan_test", 100, 100, 15.0)],
+                analyses=[dict(kind="basic", species=[0, 1, 2], cells=(0, 99), t=(0.0, 2.0))])
+
+
+CASES = {
+    "her_test": _her_test,
+    "her_pert": _her_pert,
+    "her_sets": _her_sets,
+    "her_delays": _her_delays,
+    "her_init": _her_init,
+    "turing": _turing,
+    "nan_test": _nan_test,
+}
+
+
+def build_case(name):
+    return CASES[name]()

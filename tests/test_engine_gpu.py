@@ -1,0 +1,131 @@
+"""Parity of the CUDA engine (through its C ABI) with DENSE: bit for bit in
+FP64 against DENSE's own outputs (fixtures) and the oracle; FP32+Kahan
+within a stated tolerance; status words and drop semantics."""
+
+import math
+
+import numpy as np
+import pytest
+
+from dense_b200 import engine as E
+from tests.golden.cases import build_case
+from tests.helpers import load_fixture, mismatches, run_engine, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init"]
+
+
+@pytest.mark.parametrize("name", EXACT_CASES)
+def test_fp64_bitwise_vs_dense_fixture(name):
+    want = load_fixture(name)
+    got = run_engine(name)
+    for s in range(len(build_case(name)["sets"])):
+        assert got["status_%d" % s] == 0
+    assert mismatches(want, got) == []
+
+
+@pytest.mark.parametrize("name", ["her_pert", "her_sets"])
+def test_fp64_bitwise_vs_oracle(name):
+    from oracle.pyoracle import load_oracle
+    want = run_oracle(load_oracle("her_model_2014"), name)
+    assert mismatches(want, run_engine(name)) == []
+
+
+def test_graph_replay_and_chunked_runs_match_one_launch():
+    full = run_engine("her_sets")
+    assert mismatches(full, run_engine("her_sets", graph=True)) == []
+    assert mismatches(full, run_engine("her_sets", chunks_per_call=37)) == []
+    assert mismatches(full, run_engine("her_sets", graph=True, chunks_per_call=100)) == []
+
+
+@pytest.mark.parametrize("name", ["turing", "nan_test"])
+def test_same_step_neighbour_reads_are_reported(name):
+    # neighbour averages that read the row other cells write in the same
+    # step (DENSE's cell-ordered loop) are flagged, not silently run
+    got = run_engine(name)
+    assert got["status_0"] & E.SET_ORDERED_READS
+
+
+def test_fp32_kahan_error_vs_fp64():
+    """FP32 rates with Kahan-compensated state: relative error of the final
+    state and of the oscillation periods against FP64 (60 simulated minutes,
+    200 perturbed cells)."""
+    f64 = run_engine("her_pert", precision=E.FP64)
+    f32 = run_engine("her_pert", precision=E.FP32_KAHAN)
+    a, b = f64["state_0"], f32["state_0"]
+    rel = np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-3))
+    assert rel < 2e-3, rel
+    per64, per32 = f64["a1_pers_0"], f32["a1_pers_0"]
+    ok = np.isfinite(per64) & np.isfinite(per32)
+    assert ok.sum() > 0
+    assert np.max(np.abs(per64[ok] - per32[ok]) / per64[ok]) < 2e-2
+
+
+def _her_batch(sets_params, cells=16, duration=30.0, analyses=()):
+    from dense_b200.tissue import default_graph
+    off, ids = default_graph(cells, 4)
+    sets = [E.ParameterSet(off, ids, p, duration=duration) for p in sets_params]
+    return E.Batch("her_model_2014", sets, 0.01, 0.1, list(analyses))
+
+
+def test_nan_parameter_rejects_only_that_set():
+    from dense_b200 import workloads
+    p = workloads.template_params()
+    bad = p.copy()
+    bad[3] = float("nan")
+    b = _her_batch([p, bad, p])
+    b.run()
+    b.sync()
+    st = b.status()
+    assert st[0] == 0 and st[2] == 0 and st[1] & E.SET_NAN_PARAM
+    assert np.array_equal(b.state(0), b.state(2))
+    ch, age = b.progress()
+    assert ch[1] == 0 and ch[0] == 300
+
+
+def test_concentration_check_drops_like_the_oracle():
+    """ConcentrationCheck (conccheck.hpp:25-51) with run_simulation's drop
+    (run_simulation.hpp:131-150): the set stops at the first chunk whose
+    sample leaves the bounds."""
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    from oracle.pyoracle import load_oracle
+    p = workloads.template_params()
+    mh1 = workloads.her_species("mh1")[0]
+    b = _her_batch([p, p], analyses=[E.Analysis.conccheck([mh1], 0, 16, 0.0, 30.0)])
+    b.run()
+    b.sync()
+    st = b.status()
+    ch, age = b.progress()
+    O = load_oracle("her_model_2014")
+    off, ids = default_graph(16, 4)
+    sim = O.create(off, ids, np.tile(p, (16, 1)), p, None, 0.01)
+    sim.add_conccheck(mh1, 0, 16, 0.0, 30.0)
+    a = sim.run(30.0, 0.1)
+    assert sim.status() & 1
+    assert st[0] & E.SET_DROPPED and st[1] & E.SET_DROPPED
+    assert ch[0] == a and ch[1] == a
+    b2 = _her_batch([p], analyses=[E.Analysis.conccheck([mh1], 0, 16, 0.0, 1e9)])
+    b2.run()
+    assert b2.status()[0] == 0
+
+
+def test_uneven_horizons_in_one_batch():
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    from oracle.pyoracle import load_oracle
+    O = load_oracle("her_model_2014")
+    P = workloads.log_uniform_params(3, seed=9)
+    off, ids = default_graph(12, 4)
+    durs = [5.0, 12.3, 0.0]
+    sets = [E.ParameterSet(off, ids, P[i], duration=durs[i]) for i in range(3)]
+    b = E.Batch("her_model_2014", sets, 0.01, 0.1)
+    b.run()
+    ch, age = b.progress()
+    for i in range(3):
+        sim = O.create(off, ids, np.tile(P[i], (12, 1)), P[i], None, 0.01)
+        n = sim.run(durs[i], 0.1)
+        assert ch[i] == n == math.ceil(durs[i] / 0.1)
+        assert age[i] == sim.age()
+        assert np.array_equal(b.state(i), sim.state())

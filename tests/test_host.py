@@ -1,0 +1,77 @@
+"""Host-side logic that needs no GPU: the C ABI exports, CSV reading,
+report formatting."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from dense_b200 import csvio, report
+from dense_b200.build import lib_path
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "dense_b200.h")).read()
+    return sorted(set(re.findall(r"DENSE_API [a-z_ *]+?\b(dense_[a-z_]+)\(", text)))
+
+
+@pytest.mark.parametrize("model", ["her_model_2014", "turing", "nan_test", "delay_reaction", "bz",
+                                   "briggs_rauscher"])
+def test_library_exports_every_declared_symbol(model):
+    from dense_b200.build import build_model
+    path = build_model(model)
+    lib = ctypes.CDLL(path)
+    syms = declared_symbols()
+    assert len(syms) >= 17
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+def test_model_info_matches_oracle():
+    from dense_b200.engine import load
+    from oracle.pyoracle import load_oracle
+    for model in ("her_model_2014", "turing", "nan_test"):
+        L = load(model)
+        O = load_oracle(model)
+        assert (L.num_species, L.num_reactions, L.num_delay_reactions, L.num_critical_species, L.num_params) == \
+            (O.num_species, O.num_reactions, O.num_delay_reactions, O.num_critical_species, O.num_params)
+        assert L.species == O.species and L.reactions == O.reactions
+    L = load("her_model_2014")
+    assert (L.num_species, L.num_reactions, L.num_delay_reactions, L.num_critical_species, L.num_params) == \
+        (14, 34, 8, 3, 45)
+
+
+def test_csv_trailing_value_rule():
+    # a value is emitted only at a comma (io/csvr.cpp:80-99)
+    assert csvio.read_reals("5.1, 5.2, 5.3, 5.9\n") == [5.1, 5.2, 5.3]
+    assert csvio.read_reals("1,\n2,") == [1.0, 2.0]
+    assert csvio.read_reals("1\n2,") == [12.0]
+
+
+def test_csv_comments_and_headers():
+    text = "# a comment, with commas\nname, other,\n1e-3, -2.5e2,+3,"
+    assert csvio.read_reals(text) == [1e-3, -250.0, 3.0]
+
+
+def test_csv_param_sets_partial_is_error():
+    with pytest.raises(ValueError):
+        csvio.read_param_sets("1,2,3,", 2)
+    assert csvio.read_param_sets("1,2,3,4,", 2) == [[1.0, 2.0], [3.0, 4.0]]
+
+
+def test_csv_init_conc_pads_and_truncates():
+    assert csvio.read_init_conc("1,2,", 4) == [1.0, 2.0, 0.0, 0.0]
+    assert csvio.read_init_conc("1,2,3,4,5,", 3) == [1.0, 2.0, 3.0]
+
+
+def test_report_number_format():
+    assert report.fmt(188.37427272) == "188.374"
+    assert report.fmt(0.0) == "0"
+    assert report.fmt(2999.9900000190623) == "2999.99"
+    assert report.fmt(float("nan")) == "nan"
+    assert report.fmt(-float("nan")) == "-nan"
+    assert report.fmt(1e-7) == "1e-07"
