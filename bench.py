@@ -259,7 +259,7 @@ def main():
         if k == 0:
             h2d = sum(s.num_cells * len(s.set_params) * 8 + s.nbr_offsets.nbytes + s.nbr_ids.nbytes for s in sets)
             d2h = sum(r["amps"].nbytes + r["pers"].nbytes + r["avg_peak"].nbytes + r["ncrit"].nbytes for r in res)
-    e2e_s = max(e2e_times)
+    e2e_s = max(e2e_times) if e2e_times else float("nan")
     if world > 1:
         x = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)

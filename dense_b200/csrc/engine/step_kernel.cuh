@@ -270,17 +270,20 @@ __device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& 
 
 // OscillationAnalysis::finalize (oscillation.ipp:6-26) and
 // calcAmpsAndPers for thread c's cell; also the "avg peak" of show().
-__device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc& A, int c) {
+// DENSE's sample counter restarts from its pre-finalize value for every
+// (species, cell) window and is left at the value of the last one; the
+// thread of the last cell writes that value.
+__device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc& A, int c, double samples0) {
   if (c < A.cmin || c >= A.cmax) return;
   const int n = A.nsp, m = A.cmax - A.cmin, w = A.range_steps + 1;
   const int cc = c - A.cmin;
   OscCell* cells = reinterpret_cast<OscCell*>(st + 2);
   double* windows = st + 2 + static_cast<size_t>(n) * m * kOscCellDoubles;
-  const double samples0 = st[0];
+  double samples = samples0;
   for (int i = 0; i < n; ++i) {
     OscCell o = cells[static_cast<size_t>(i) * m + cc];
     double* win = windows + static_cast<size_t>(i) * w * m + cc;
-    double samples = samples0;
+    samples = samples0;
     for (;;) {
       DevQueue q{static_cast<long>(o.start), static_cast<long>(o.end), static_cast<long>(o.current), w};
       if (!(q.get_size() >= (A.range_steps / 2) && o.live > 0.0)) break;
@@ -294,6 +297,7 @@ __device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc
     o.avg_peak = (o.num_peaks != 0.0) ? o.peak_sum / o.num_peaks : o.peak_sum;
     cells[static_cast<size_t>(i) * m + cc] = o;
   }
+  if (cc == m - 1) st[0] = samples;
 }
 
 // ---------------------------------------------------------------- kernel
@@ -463,13 +467,15 @@ __global__ void __launch_bounds__(256, 1) dense_step_kernel(const StepArgs a) {
     }
   }
   if (err) atomicOr(&s_flags, err << 1);
+  // pre-finalize sample counters, read before any thread finalizes
+  if (c < a.n_analyses) s_samples[c] = anl[a.analyses[c].off];
   __syncthreads();
   const int status = pg.status | (dropped ? kSetDropped : 0) | (s_flags >> 1);
   const bool finish = !dropped && chunk >= sd.n_chunks;
   if (finish) {
     for (int ai = 0; ai < a.n_analyses; ++ai) {
       const AnalysisDesc& A = a.analyses[ai];
-      if (A.kind == kOscillation) osc_cell_finalize(anl + A.off, A, c);
+      if (A.kind == kOscillation) osc_cell_finalize(anl + A.off, A, c, s_samples[ai]);
     }
   }
   if (c == 0) {
