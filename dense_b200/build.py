@@ -37,6 +37,7 @@ UNITS = {
     "kernels_fp64.cu": ["--fmad=false"],
     "kernels_fp32.cu": [],
     "engine_api.cu": [],
+    "noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -52,6 +52,7 @@ extern "C" {
 #define DENSE_ERR_CUDA 2        /* CUDA runtime failure */
 #define DENSE_ERR_MEMORY 3      /* device allocation failed */
 #define DENSE_ERR_UNSUPPORTED 4 /* a batch the engine does not run */
+#define DENSE_ERR_SCRATCH_TOO_SMALL 5 /* dense_simulate_noalloc: the batch exceeds its fixed scratch */
 
 /* per-set status bits (dense_engine_status) */
 #define DENSE_SET_OK 0
@@ -169,6 +170,30 @@ DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int6
 DENSE_API int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D);
 
 DENSE_API int dense_engine_destroy(dense_engine* e);
+
+/* No counterpart in DENSE: an addition of this library for callers that may
+   not allocate device memory -- code running inside a framework that owns
+   the GPU's whole memory through its own pool, or a service loop that must
+   not call cudaMalloc after start-up because it can synchronize the device.
+
+   Runs an FP64 batch without analyses from host inputs to the final lag-0
+   state (final_state: the sets' [num_species][num_cells] blocks one after
+   another; status: [num_sets] DENSE_SET_* words, or NULL) and returns when
+   the results are on the host.  It allocates nothing: every device buffer
+   lives in one fixed 16 MiB array inside this library, which every GPU that
+   loads the library holds until the process exits.  Limits: at most 64 sets
+   of at most 256 cells, and the batch's descriptors, parameters, neighbour
+   lists, state and history rings must fit in 16 MiB; a larger batch returns
+   DENSE_ERR_SCRATCH_TOO_SMALL.  precision must be DENSE_FP64 and
+   num_analyses 0 (DENSE_ERR_UNSUPPORTED otherwise).
+   The first call on a device looks up the array's device address (with that
+   device current); make that first call before any stream capture on the
+   device.  All calls share the array: calls that overlap on the GPU (two
+   host threads, or two streams not ordered against each other) race and
+   must not be made.  Every region a call reads is written by the same call
+   first, so the array's previous contents never leak into results. */
+DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int num_sets, const dense_set_desc* sets,
+                                     double* final_state, int32_t* status, void* stream);
 
 #ifdef __cplusplus
 }
