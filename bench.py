@@ -186,6 +186,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--analyses", default="oscillation", choices=["oscillation", "none"],
+                    help="the workload's analyses: Oscillation(mh1) every 0.1 min, or none")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -201,6 +203,8 @@ def main():
 
     precision = E.FP64 if a.precision == "fp64" else E.FP32_KAHAN
     sets, analyses = build_workload(a.sets, a.minutes, seed=2 + rank)
+    if a.analyses == "none":
+        analyses = []
     batch = E.Batch("her_model_2014", sets, 0.01, 0.1, analyses, precision=precision, device=local)
     info = batch.info()
     total_chunks = int(math.ceil(a.minutes / 0.1))
@@ -252,13 +256,16 @@ def main():
         t0 = time.perf_counter()
         b = E.Batch("her_model_2014", sets, 0.01, 0.1, analyses, precision=precision, device=local)
         b.run(-1)
-        res = [b.oscillation(0, i) for i in range(len(sets))]
+        if analyses:
+            res = [b.oscillation(0, i) for i in range(len(sets))]
+        else:
+            res = [{"state": b.state(i)} for i in range(len(sets))]
         b.close()
         barrier()
         e2e_times.append(time.perf_counter() - t0)
         if k == 0:
             h2d = sum(s.num_cells * len(s.set_params) * 8 + s.nbr_offsets.nbytes + s.nbr_ids.nbytes for s in sets)
-            d2h = sum(r["amps"].nbytes + r["pers"].nbytes + r["avg_peak"].nbytes + r["ncrit"].nbytes for r in res)
+            d2h = sum(sum(v.nbytes for v in r.values() if hasattr(v, "nbytes")) for r in res)
     e2e_s = max(e2e_times) if e2e_times else float("nan")
     if world > 1:
         x = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -287,8 +294,9 @@ def main():
             "warmup": a.warmup, "ms_per_step": total_ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if precision == E.FP64 else "f32+kahan", "data": "synthetic",
             "config": {"workload": "her_model_2014: %d parameter sets (template x exp(U(ln .5, ln 2)) per set), "
-                                   "200 cells each (-c 200 -w 4), dt 0.01 min, %g min, Oscillation(mh1, all "
-                                   "cells, window 4 min) every 0.1 min" % (a.sets, a.minutes),
+                                   "200 cells each (-c 200 -w 4), dt 0.01 min, %g min, %s"
+                                   % (a.sets, a.minutes, "Oscillation(mh1, all cells, window 4 min) every 0.1 min"
+                                      if analyses else "no analyses"),
                        "sets_per_gpu": a.sets, "step": "one launch advancing every set %d chunks (%g min)"
                        % (per_step, per_step * 0.1), "l2": "inputs larger than L2 (history rings + "
                        "windows %.0f MB per GPU)" % (info["device_bytes"] / 1e6),

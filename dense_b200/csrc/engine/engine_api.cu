@@ -144,6 +144,12 @@ struct dense_engine {
 namespace {
 
 // ring sizes and traced depths for one set
+int next_pow2(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
 int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<double>& cell_params) {
   const int n = in.num_cells;
   SetDesc& d = plan.d;
@@ -170,13 +176,16 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
       return fail(DENSE_ERR_INVALID, "ring size of species " + std::to_string(sp) + " is not a positive int");
     d.S[sp] = static_cast<int>(v);
   }
-  // per-cell parameters, [NP][n] for the device; NaN rates/delays reject
-  // the set, as DENSE's getRate/getDelay throw (sim/base.hpp:398-412)
-  cell_params.resize(static_cast<size_t>(NUM_PARAMS) * n);
-  for (int c = 0; c < n; ++c) {
+  // parameters for the device: one row [NP] when every cell uses the set's
+  // parameters, else [NP][n]; NaN rates/delays reject the set, as DENSE's
+  // getRate/getDelay throw (sim/base.hpp:398-412)
+  const int pcols = in.cell_params ? n : 1;
+  d.param_stride = in.cell_params ? n : 0;
+  cell_params.resize(static_cast<size_t>(NUM_PARAMS) * pcols);
+  for (int c = 0; c < pcols; ++c) {
     const double* p = in.cell_params ? in.cell_params + static_cast<size_t>(c) * NUM_PARAMS : in.set_params;
     for (int i = 0; i < NUM_PARAMS; ++i) {
-      cell_params[static_cast<size_t>(i) * n + c] = p[i];
+      cell_params[static_cast<size_t>(i) * pcols + c] = p[i];
       if (i < NUM_REACTIONS + NUM_DELAY_REACTIONS && std::isnan(p[i])) plan.status |= kSetNanParam;
     }
   }
@@ -190,7 +199,7 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
   // cells sharing the set's parameters all read the same lags: trace one
   const int traced = in.cell_params ? n : 1;
   for (int c = 0; c < traced; ++c) {
-    for (int i = 0; i < NUM_PARAMS; ++i) prm[i] = cell_params[static_cast<size_t>(i) * n + c];
+    for (int i = 0; i < NUM_PARAMS; ++i) prm[i] = cell_params[static_cast<size_t>(i) * pcols + c];
     for (int pass = 0; pass < 4; ++pass) {
       for (int sp = 0; sp < NUM_SPECIES; ++sp) conc[sp] = pass == 0 ? 0.0 : (pass == 1 ? 1.0 : 0.37 * (sp + pass));
       LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad};
@@ -206,8 +215,9 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
     int depth = 0;
     if (own_max[sp] >= 1) depth = own_max[sp] + 1;
     if (nbr_max[sp] >= 0) depth = std::max(depth, nbr_max[sp] + 2);
-    depth = std::min(depth, d.S[sp] + 1);
-    d.D[sp] = depth;
+    // a power of two, so a row is (step - lag) & (D - 1)
+    d.D[sp] = depth > 0 ? next_pow2(depth) : 0;
+    depth = d.D[sp];
     d.ring_off[sp] = off;
     off += static_cast<int64_t>(depth) * n;
   }
@@ -261,7 +271,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   CUDA_TRY(cudaSetDevice(run->device));
 
   // ---- analyses
-  int min_cells = kMaxCellsPerSet + 1;
+  int min_cells = kStepThreads + 1;
   for (int s = 0; s < num_sets; ++s) min_cells = std::min(min_cells, in_sets[s].num_cells);
   int64_t anl_block = 0;
   for (int ai = 0; ai < run->num_analyses; ++ai) {
@@ -298,7 +308,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       if (!(rs < 1e6)) return fail(DENSE_ERR_UNSUPPORTED, "oscillation window too long");
       A.range_steps = static_cast<int>(rs);
       A.interval = in.anlys_intvl;
-      anl_block += 2 + m * A.nsp * kOscCellDoubles + static_cast<int64_t>(A.nsp) * (A.range_steps + 1) * m;
+      anl_block += 2 + m * A.nsp * kOscFields + static_cast<int64_t>(A.nsp) * (A.range_steps + 1) * m;
     } else if (in.kind == DENSE_ANALYSIS_CONCCHECK) {
       A.lo = in.lower;
       A.hi = in.upper;
@@ -314,14 +324,14 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   std::vector<double> params_all, conc_all(static_cast<size_t>(num_sets) * NUM_SPECIES, 0.0);
   std::vector<int> off_all, idx_all;
   int64_t cells_total = 0, ring_total = 0;
-  int max_cells = 0;
+  int max_cells = 0, max_edges = 0;
   e->sets.resize(num_sets);
   e->init_status.resize(num_sets);
   std::vector<double> cp;
   for (int s = 0; s < num_sets; ++s) {
     const dense_set_desc& in = in_sets[s];
     const std::string where = "set " + std::to_string(s) + ": ";
-    if (in.num_cells <= 0 || in.num_cells > 256)
+    if (in.num_cells <= 0 || in.num_cells > kStepThreads)
       return fail(DENSE_ERR_UNSUPPORTED, where + "1..256 cells per set are supported");
     if (!in.nbr_offsets || !in.nbr_ids || !in.set_params) return fail(DENSE_ERR_INVALID, where + "null input");
     if (!(in.duration >= 0.0)) return fail(DENSE_ERR_INVALID, where + "negative duration");
@@ -344,6 +354,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     if (!(chunks < 2147483647.0)) return fail(DENSE_ERR_INVALID, where + "too many chunks");
     d.n_chunks = static_cast<int>(std::ceil(chunks));
     d.steps_per_chunk = steps_per_chunk;
+    d.param_base = static_cast<int64_t>(params_all.size());
     d.cell_base = cells_total;
     d.nbr_base = static_cast<int64_t>(off_all.size());
     d.ring_base = ring_total;
@@ -362,6 +373,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     ring_total += ring_elems(d);
     ring_total = (ring_total + 31) & ~int64_t(31);
     max_cells = std::max(max_cells, n);
+    max_edges = std::max(max_edges, in.nbr_offsets[n]);
     e->total_cell_steps += static_cast<int64_t>(n) * d.n_chunks * steps_per_chunk;
     e->sets[s] = d;
   }
@@ -372,7 +384,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   int rc;
   if ((rc = e->d_sets.alloc(sizeof(SetDesc) * num_sets))) return rc;
   if ((rc = e->d_prog.alloc(sizeof(SetProgress) * num_sets))) return rc;
-  if ((rc = e->d_params.alloc(sizeof(double) * params_all.size()))) return rc;
+  if ((rc = e->d_params.alloc(tsz * params_all.size()))) return rc;
   if ((rc = e->d_nbr_off.alloc(sizeof(int) * off_all.size()))) return rc;
   if ((rc = e->d_nbr_idx.alloc(sizeof(int) * idx_all.size()))) return rc;
   if ((rc = e->d_state.alloc(tsz * 2 * NUM_SPECIES * cells_total))) return rc;
@@ -381,7 +393,15 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   if ((rc = e->d_init_conc.alloc(sizeof(double) * conc_all.size()))) return rc;
   if ((rc = e->d_init_status.alloc(sizeof(int) * num_sets))) return rc;
   CUDA_TRY(cudaMemcpyAsync(e->d_sets.p, e->sets.data(), sizeof(SetDesc) * num_sets, cudaMemcpyHostToDevice, e->stream));
-  CUDA_TRY(cudaMemcpyAsync(e->d_params.p, params_all.data(), sizeof(double) * params_all.size(), cudaMemcpyHostToDevice, e->stream));
+  std::vector<float> params_f;
+  if (run->precision == DENSE_FP64) {
+    CUDA_TRY(cudaMemcpyAsync(e->d_params.p, params_all.data(), sizeof(double) * params_all.size(),
+                             cudaMemcpyHostToDevice, e->stream));
+  } else {
+    params_f.assign(params_all.begin(), params_all.end());
+    CUDA_TRY(cudaMemcpyAsync(e->d_params.p, params_f.data(), sizeof(float) * params_f.size(),
+                             cudaMemcpyHostToDevice, e->stream));
+  }
   CUDA_TRY(cudaMemcpyAsync(e->d_nbr_off.p, off_all.data(), sizeof(int) * off_all.size(), cudaMemcpyHostToDevice, e->stream));
   if (!idx_all.empty())
     CUDA_TRY(cudaMemcpyAsync(e->d_nbr_idx.p, idx_all.data(), sizeof(int) * idx_all.size(), cudaMemcpyHostToDevice, e->stream));
@@ -394,7 +414,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   StepArgs& a = e->args;
   a.sets = static_cast<const SetDesc*>(e->d_sets.p);
   a.prog = static_cast<SetProgress*>(e->d_prog.p);
-  a.params = static_cast<const double*>(e->d_params.p);
+  a.params = e->d_params.p;
   a.nbr_off = static_cast<const int*>(e->d_nbr_off.p);
   a.nbr_idx = static_cast<const int*>(e->d_nbr_idx.p);
   a.state = e->d_state.p;
@@ -407,7 +427,16 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   a.interval = interval;
   a.chunk_count = -1;
   a.block_threads = std::max(32, (max_cells + 31) / 32 * 32);
-  e->smem = a.n_analyses > 0 ? sizeof(double) * NUM_SPECIES * a.block_threads : 0;
+  // shared memory: sampled state (with analyses), truncated delays, and
+  // each set's neighbour ids when the largest list fits
+  size_t smem = (a.n_analyses > 0 ? sizeof(double) * NUM_SPECIES * a.block_threads : 0) +
+                sizeof(int) * NUM_DELAY_REACTIONS * a.block_threads;
+  const size_t csr_bytes = sizeof(int) * max_edges;
+  const size_t smem_cap = a.block_threads <= 224 ? 100000 : 200000;
+  a.csr_in_smem = smem + csr_bytes <= smem_cap ? 1 : 0;
+  if (a.csr_in_smem) smem += csr_bytes;
+  if (smem > smem_cap) return fail(DENSE_ERR_UNSUPPORTED, "shared memory need of the batch too large");
+  e->smem = smem;
 
   rc = dense_engine_reset(e.get(), nullptr);
   if (rc != DENSE_OK) return rc;
@@ -532,7 +561,7 @@ static int read_analysis_block(dense_engine* e, int analysis, int set, int kind,
   int64_t len;
   const int64_t m = (*A)->cmax - (*A)->cmin, nsp = (*A)->nsp;
   if (kind == kBasic) len = 3 * nsp + 2 + 3 * m * nsp;
-  else len = 2 + m * nsp * kOscCellDoubles;
+  else len = 2 + m * nsp * kOscFields;
   blk.resize(len);
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaDeviceSynchronize());
@@ -556,12 +585,15 @@ int dense_engine_read_basic(dense_engine* e, int analysis, int set, double* mins
   }
   if (samples) *samples = static_cast<int>(b[3 * n]);
   if (time) *time = b[3 * n + 1];
-  const double* cb = b.data() + 3 * n + 2;
-  for (size_t k = 0; k < mn; ++k) {
-    if (cell_mins) cell_mins[k] = cb[k];
-    if (cell_maxs) cell_maxs[k] = cb[mn + k];
-    if (cell_sums) cell_sums[k] = cb[2 * mn + k];
-  }
+  const double* cb = b.data() + 3 * n + 2;  // [n][m] on the device, [m][n] for the caller
+  const int m = A->cmax - A->cmin;
+  for (int c = 0; c < m; ++c)
+    for (int i = 0; i < n; ++i) {
+      const size_t dev = static_cast<size_t>(i) * m + c, out = static_cast<size_t>(c) * n + i;
+      if (cell_mins) cell_mins[out] = cb[dev];
+      if (cell_maxs) cell_maxs[out] = cb[mn + dev];
+      if (cell_sums) cell_sums[out] = cb[2 * mn + dev];
+    }
   return DENSE_OK;
 }
 
@@ -572,12 +604,12 @@ int dense_engine_read_oscillation(dense_engine* e, int analysis, int set, double
   int rc = read_analysis_block(e, analysis, set, kOscillation, b, &A);
   if (rc) return rc;
   const size_t k = static_cast<size_t>(A->cmax - A->cmin) * A->nsp;
-  const OscCell* cells = reinterpret_cast<const OscCell*>(b.data() + 2);
+  const double* f = b.data() + 2;  // [field][species][cell]
   for (size_t i = 0; i < k; ++i) {
-    if (amps) amps[i] = cells[i].amp;
-    if (periods) periods[i] = cells[i].per;
-    if (avg_peaks) avg_peaks[i] = cells[i].avg_peak;
-    if (num_crit) num_crit[i] = static_cast<int>(cells[i].ncrit);
+    if (amps) amps[i] = f[kOscAmp * k + i];
+    if (periods) periods[i] = f[kOscPer * k + i];
+    if (avg_peaks) avg_peaks[i] = f[kOscAvgPeak * k + i];
+    if (num_crit) num_crit[i] = static_cast<int>(f[kOscNcrit * k + i]);
   }
   if (samples) *samples = static_cast<int>(b[0]);
   if (time) *time = b[1];

@@ -15,7 +15,7 @@ constexpr int kNR = NUM_REACTIONS;
 constexpr int kND = NUM_DELAY_REACTIONS;
 constexpr int kNP = NUM_PARAMS;
 constexpr int kMaxAnalyses = 8;
-constexpr int kMaxCellsPerSet = 1024;  // one thread per cell, one CTA per set
+constexpr int kStepThreads = 256;  // one thread per cell, one CTA per set: at most 256 cells
 
 // Per-set status bits (also the public DENSE_SET_* values).
 enum : int {
@@ -42,33 +42,34 @@ struct AnalysisDesc {
   int64_t off;          // offset of this analysis' state inside a set's block
 };
 
-// Layout of one analysis' per-set state (doubles unless noted), relative to
+// Layout of one analysis' per-set state (doubles), relative to
 // AnalysisDesc::off.  n = nsp, m = cmax - cmin, w = range_steps + 1.
-//  Basic:       mins[n] maxs[n] sums[n] samples time | cmins[m][n] cmaxs[m][n] csums[m][n]
-//  Oscillation: samples time | per (s, c): OscCell (as doubles) | window[s][w][m]
+//  Basic:       mins[n] maxs[n] sums[n] samples time | cmins[n][m] cmaxs[n][m] csums[n][m]
+//  Oscillation: samples time | field[kOscFields][n][m] | window[n][w][m]
 //  ConcCheck:   time
-struct OscCell {
-  double start, end, current;   // queue indices (core/queue.hpp)
-  double live;                  // number of values in the window
-  double last_time, last_conc, last_peak, ncrit;
-  double t_m2, t_m1;            // times of crit points m-3 and m-2
-  double peak_sum, trough_sum, num_peaks, num_troughs, cycle_sum, cycles;
-  double amp, per, avg_peak;    // results, written by finalize
+enum OscField : int {
+  kOscStart, kOscEnd, kOscCurrent,  // queue indices (core/queue.hpp)
+  kOscLive,                         // values in the window
+  kOscLastTime, kOscLastConc, kOscLastPeak, kOscNcrit,
+  kOscTm2, kOscTm1,                 // times of critical points ncrit-3 and ncrit-2
+  kOscPeakSum, kOscTroughSum, kOscNumPeaks, kOscNumTroughs, kOscCycleSum, kOscCycles,
+  kOscAmp, kOscPer, kOscAvgPeak,    // results, written by finalize
+  kOscFields
 };
-constexpr int kOscCellDoubles = sizeof(OscCell) / sizeof(double);
 
 // One parameter set of the batch.
 struct SetDesc {
   int n_cells;
   int n_chunks;          // analysis chunks of this set's horizon
   int steps_per_chunk;   // (int)(interval / dt)
-  int pad0;
+  int param_stride;      // 0: one parameter row for every cell; n_cells: [NP][n] per cell
+  int64_t param_base;    // first double of this set's parameters
   int64_t cell_base;     // first cell of this set in the per-cell arrays
   int64_t nbr_base;      // offset of this set's CSR row offsets (n_cells + 1)
   int64_t ring_base;     // first element of this set's history block
   int64_t anl_base;      // first double of this set's analysis block
   int S[kNS];            // DENSE ring size per species (baby_cl.cpp:10)
-  int D[kNS];            // staged history depth (0: lag-0 only, kept in registers)
+  int D[kNS];            // staged history depth, a power of two (0: lag-0 only, kept in registers)
   int64_t ring_off[kNS]; // offset of each staged ring inside the set's block
 };
 
@@ -85,7 +86,7 @@ struct SetProgress {
 struct StepArgs {
   const SetDesc* sets;
   SetProgress* prog;
-  const double* params;     // per set: [NP][n_cells]
+  const void* params;       // per set, in the batch's precision: [NP] (param_stride 0) or [NP][n_cells]
   const int* nbr_off;       // per set: n_cells + 1 absolute offsets into nbr_idx
   const int* nbr_idx;       // neighbour cell ids, local to the set, ascending
   void* state;              // per set: [NS][n_cells] lag-0 state (T), then [NS][n_cells] Kahan terms
@@ -98,6 +99,7 @@ struct StepArgs {
   double interval;
   int chunk_count;          // chunks to run in this launch (-1: to the end)
   int block_threads;
+  int csr_in_smem;          // copy each set's neighbour ids into shared memory
 };
 
 }  // namespace dense_b200

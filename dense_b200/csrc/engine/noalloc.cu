@@ -196,7 +196,9 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
       int depth = 0;
       if (own_max[sp] >= 1) depth = own_max[sp] + 1;
       if (nbr_max[sp] >= 0 && nbr_max[sp] + 2 > depth) depth = nbr_max[sp] + 2;
-      if (depth > d.S[sp] + 1) depth = d.S[sp] + 1;
+      int pow2 = depth > 0 ? 1 : 0;
+      while (pow2 < depth) pow2 <<= 1;
+      depth = pow2;
       d.D[sp] = depth;
       d.ring_off[sp] = off;
       off += static_cast<int64_t>(depth) * n;
@@ -206,6 +208,8 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
     d.n_chunks = static_cast<int>(std::ceil(chunks));
     d.steps_per_chunk = static_cast<int>(steps_d);
     d.cell_base = cells_total;
+    d.param_base = cells_total * NUM_PARAMS;  // [NP][n] per set
+    d.param_stride = n;
     d.nbr_base = cells_total + si;  // offsets region: n + 1 entries per set
     d.ring_base = ring_total;
     d.anl_base = 0;
@@ -263,7 +267,7 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   StepArgs a{};
   a.sets = reinterpret_cast<const SetDesc*>(base + o_sets);
   a.prog = reinterpret_cast<SetProgress*>(base + o_prog);
-  a.params = reinterpret_cast<const double*>(base + o_params);
+  a.params = base + o_params;
   a.nbr_off = reinterpret_cast<const int*>(base + o_off);
   a.nbr_idx = reinterpret_cast<const int*>(base + o_idx);
   a.state = base + o_state;
@@ -277,7 +281,8 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   a.block_threads = max_cells < 32 ? 32 : (max_cells + 31) / 32 * 32;
   NA_TRY(launch_init_fp64(a, reinterpret_cast<const double*>(base + o_conc),
                           reinterpret_cast<const int*>(base + o_status), s));
-  NA_TRY(launch_step_fp64(a, 0, s));
+  a.csr_in_smem = 0;
+  NA_TRY(launch_step_fp64(a, sizeof(int) * NUM_DELAY_REACTIONS * a.block_threads, s));
 
   // ---- results to the caller's buffers
   size_t out_off = 0;

@@ -29,92 +29,115 @@
 
 namespace dense_b200 {
 
+// What getDelay returns: the delay reaction and this cell's delay truncated
+// to int (the conversion DENSE applies when the delay is passed on as
+// getCon's or calculateNeighborAvg's `int delay`, sim/base.hpp:68-71).
+// Used as a number it converts to the delay value itself.
+template <typename T>
+struct DelayArg {
+  const T* prm;
+  int pstride;
+  int dr;
+  int k;
+  __device__ __forceinline__ operator T() const { return prm[(kNR + dr) * pstride]; }
+};
+
 template <typename T>
 struct DeviceContext {
-  const T* cur;            // this cell's lag-0 state [NS]
-  const T* prm;            // this cell's parameters [NP]
-  T* const* ring;          // per species ring base for this set (nullptr: unstaged)
-  const int* head;         // per species slot holding lag 0
-  const int* S;            // DENSE ring sizes (shared memory)
-  const int* D;            // staged depths (shared memory)
-  const int* nbr;          // neighbour ids of this cell (global)
+  const T* cur;            // this cell's lag-0 state [NS] (registers)
+  const T* prm;            // parameters: shared row (pstride 1) or this cell's column (pstride n)
+  int pstride;
+  const int* kd;           // truncated delays, kd[d * kd_stride] (shared)
+  int kd_stride;
+  const int* S;            // DENSE ring sizes (shared)
+  const int* mask;         // staged depth - 1 per species, -1 unstaged (shared)
+  const int64_t* roff;     // ring offset per species (shared)
+  T* ring;                 // this set's ring block
+  int step;                // Euler steps done: lag 0 sits in row step & mask
+  const int* nbr;          // this cell's neighbour ids (shared, or global for large lists)
   int nnbr;
   int n_cells;
   int cell;
   int* err;
 
-  // Context::getCon(sp) -> get_concentration(cell, sp, 1) -> row_at(sp, 0).
-  __device__ __forceinline__ T getCon(specie_id sp) const { return cur[sp]; }
-
-  // Context::getCon(sp, delay) -> row_at(sp, 1 - delay)[cell]
-  // (sim/base.hpp:419-422, determ.hpp:77-79).
-  __device__ __forceinline__ T getCon(specie_id sp, int k) const {
+  __device__ __forceinline__ T own(specie_id sp, int k) const {
     const int s = S[sp];
     int lag = k - 1;
     if (lag < 0) lag += s;
-    else if (lag >= s) lag -= s;
-    if (k < 0 || k > s + 1) {
-      *err |= kSetBadDelay;
+    if (static_cast<unsigned>(k) > static_cast<unsigned>(s)) {  // k < 0 or k > S: rare
+      if (k < 0 || k > s + 1) *err |= kSetBadDelay;
       lag = ((k - 1) % s + s) % s;
     }
     if (lag == 0) return cur[sp];
-    const int d = D[sp];
-    if (lag >= d) {
+    const int m = mask[sp];
+    if (lag > m) {
       *err |= kSetUnstagedLag;
       return T(0);
     }
-    int slot = head[sp] - lag;
-    if (slot < 0) slot += d;
-    return ring[sp][static_cast<size_t>(slot) * n_cells + cell];
+    return ring[roff[sp] + static_cast<int64_t>((step - lag) & m) * n_cells + cell];
   }
 
-  // Context::calculateNeighborAvg -> calculate_neighbor_average
-  // (determ.hpp:81-89): ascending neighbour order, sum / count, NaN -> 0.
-  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, int k = 0) const {
+  __device__ __forceinline__ T nbr_avg(specie_id sp, int k) const {
     const int s = S[sp];
     int lag = k;
-    if (lag >= s) lag -= s;
-    if (k < 0 || k > s) {
-      *err |= kSetBadDelay;
+    if (static_cast<unsigned>(k) >= static_cast<unsigned>(s)) {  // k < 0 or k >= S: rare
+      if (k < 0 || k > s) *err |= kSetBadDelay;
       lag = (k % s + s) % s;
     }
-    const int d = D[sp];
-    if (lag + 1 >= d) {
+    const int m = mask[sp];
+    // lag S-1 is the row other cells write in this very step (DENSE's
+    // cell-ordered loop reads new values of lower-numbered neighbours);
+    // this schedule does not run such reads
+    if (lag >= m || lag == s - 1) {
       *err |= (lag == s - 1) ? kSetOrderedReads : kSetUnstagedLag;
       return T(0);
     }
-    int slot = head[sp] - lag;
-    if (slot < 0) slot += d;
-    const T* row = ring[sp] + static_cast<size_t>(slot) * n_cells;
+    const T* row = ring + roff[sp] + static_cast<int64_t>((step - lag) & m) * n_cells;
     T sum = T(0);
     for (int e = 0; e < nnbr; ++e) sum += row[nbr[e]];
     T avg = sum / static_cast<T>(nnbr);
     return isnan(avg) ? T(0) : avg;
   }
 
+  // Context::getCon(sp) -> get_concentration(cell, sp, 1) -> row_at(sp, 0).
+  __device__ __forceinline__ T getCon(specie_id sp) const { return cur[sp]; }
+  // Context::getCon(sp, delay) -> row_at(sp, 1 - delay)[cell]
+  // (sim/base.hpp:419-422, determ.hpp:77-79): lag (k - 1) mod S.
+  __device__ __forceinline__ T getCon(specie_id sp, int k) const { return own(sp, k); }
+  __device__ __forceinline__ T getCon(specie_id sp, DelayArg<T> d) const { return own(sp, d.k); }
+  // Context::calculateNeighborAvg -> calculate_neighbor_average
+  // (determ.hpp:81-89): row_at(sp, -delay), lag k mod S, ascending
+  // neighbour order, sum / count, NaN -> 0.
+  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, int k = 0) const { return nbr_avg(sp, k); }
+  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, DelayArg<T> d) const { return nbr_avg(sp, d.k); }
   // Context::getRate / getDelay / getCritVal (sim/base.hpp:393-412).  NaN
   // rates and delays are rejected when the batch is created.
-  __device__ __forceinline__ T getRate(reaction_id r) const { return prm[r]; }
-  __device__ __forceinline__ T getDelay(delay_reaction_id d) const { return prm[kNR + d]; }
-  __device__ __forceinline__ T getCritVal(critspecie_id c) const { return prm[kNR + kND + c]; }
+  __device__ __forceinline__ T getRate(reaction_id r) const { return prm[r * pstride]; }
+  __device__ __forceinline__ DelayArg<T> getDelay(delay_reaction_id d) const {
+    return DelayArg<T>{prm, pstride, static_cast<int>(d), kd[d * kd_stride]};
+  }
+  __device__ __forceinline__ T getCritVal(critspecie_id c) const { return prm[(kNR + kND + c) * pstride]; }
 };
 
 // ------------------------------------------------------------ analyses
+// All per-cell analysis state is structure-of-arrays over the analysed
+// cells, so the threads of a warp touch consecutive doubles.
+
 // BasicAnalysis::update (basic.ipp:22-36), per-cell part: thread c updates
-// its own row.  std::min(x, m) = (m < x) ? m : x, std::max(x, M) =
+// its own column.  std::min(x, m) = (m < x) ? m : x, std::max(x, M) =
 // (x < M) ? M : x, NaN behaviour kept.
 __device__ __forceinline__ void basic_cell_update(double* st, const AnalysisDesc& A,
                                                   const double* s_vals, int blk, int c) {
   const int n = A.nsp;
   const int m = A.cmax - A.cmin;
   if (c < A.cmin || c >= A.cmax) return;
-  double* cmins = st + 3 * n + 2;
+  double* cmins = st + 3 * n + 2;  // [n][m]
   double* cmaxs = cmins + static_cast<size_t>(m) * n;
   double* csums = cmaxs + static_cast<size_t>(m) * n;
   const int cc = c - A.cmin;
   for (int i = 0; i < n; ++i) {
     const double x = s_vals[A.sp[i] * blk + c];
-    const size_t k = static_cast<size_t>(cc) * n + i;
+    const size_t k = static_cast<size_t>(i) * m + cc;
     const double mn = cmins[k], mx = cmaxs[k];
     cmins[k] = (mn < x) ? mn : x;
     cmaxs[k] = (x < mx) ? mx : x;
@@ -144,62 +167,68 @@ __device__ __forceinline__ void basic_range_fold(double* st, const AnalysisDesc&
   }
 }
 
-// Queue (core/queue.hpp:29-88) over a window slice of `w` rows.
-struct DevQueue {
-  long start, end, current, size;
-  __device__ __forceinline__ long get_size() const { return (size + end - start) % size + 1; }
+// One (species, cell) of an OscillationAnalysis: field k lives at
+// p[k * stride].  The queue indices follow core/queue.hpp:29-88; the
+// critical-point fields keep what calcAmpsAndPers (oscillation.ipp:167-185)
+// needs: every point but the last is final and already folded into the
+// sums, in index order.
+struct OscRef {
+  double* p;
+  size_t stride;
+  __device__ __forceinline__ double& f(int k) const { return p[k * stride]; }
 };
 
-// OscillationAnalysis::addCritPoint (oscillation.ipp:129-144), keeping the
-// sums calcAmpsAndPers (oscillation.ipp:167-185) needs in index order:
-// every point but the last is final, so it is folded in when the next one
-// is appended.
-__device__ __forceinline__ void osc_fold_last(OscCell& o) {
-  if (o.ncrit < 1) return;
-  if (o.last_peak != 0.0) {
-    o.peak_sum = o.peak_sum + o.last_conc;
-    o.num_peaks += 1.0;
+// Queue::getSize with start/end/size as DENSE computes it.
+__device__ __forceinline__ long q_size(long start, long end, long size) { return (size + end - start) % size + 1; }
+
+__device__ __forceinline__ void osc_fold_last(const OscRef& o) {
+  const double ncrit = o.f(kOscNcrit);
+  if (ncrit < 1) return;
+  if (o.f(kOscLastPeak) != 0.0) {
+    o.f(kOscPeakSum) = o.f(kOscPeakSum) + o.f(kOscLastConc);
+    o.f(kOscNumPeaks) += 1.0;
   } else {
-    o.trough_sum = o.trough_sum + o.last_conc;
-    o.num_troughs += 1.0;
+    o.f(kOscTroughSum) = o.f(kOscTroughSum) + o.f(kOscLastConc);
+    o.f(kOscNumTroughs) += 1.0;
   }
-  if (o.ncrit - 1 >= 2) {
-    o.cycles += 1.0;
-    o.cycle_sum = o.cycle_sum + (o.last_time - o.t_m2);
+  if (ncrit - 1 >= 2) {
+    o.f(kOscCycles) += 1.0;
+    o.f(kOscCycleSum) = o.f(kOscCycleSum) + (o.f(kOscLastTime) - o.f(kOscTm2));
   }
 }
 
-__device__ __forceinline__ void osc_add_crit(OscCell& o, double t, double conc, bool peak) {
-  if (o.ncrit > 0) {
-    const bool prev_peak = o.last_peak != 0.0;
+// OscillationAnalysis::addCritPoint (oscillation.ipp:129-144).
+__device__ __forceinline__ void osc_add_crit(const OscRef& o, double t, double conc, bool peak) {
+  if (o.f(kOscNcrit) > 0) {
+    const bool prev_peak = o.f(kOscLastPeak) != 0.0;
     if (prev_peak == peak) {
-      if (peak ? (conc >= o.last_conc) : (conc <= o.last_conc)) {
-        o.last_time = t;
-        o.last_conc = conc;
+      if (peak ? (conc >= o.f(kOscLastConc)) : (conc <= o.f(kOscLastConc))) {
+        o.f(kOscLastTime) = t;
+        o.f(kOscLastConc) = conc;
       }
       return;
     }
     osc_fold_last(o);
-    o.t_m2 = o.t_m1;
-    o.t_m1 = o.last_time;
+    o.f(kOscTm2) = o.f(kOscTm1);
+    o.f(kOscTm1) = o.f(kOscLastTime);
   }
-  o.last_time = t;
-  o.last_conc = conc;
-  o.last_peak = peak ? 1.0 : 0.0;
-  o.ncrit += 1.0;
+  o.f(kOscLastTime) = t;
+  o.f(kOscLastConc) = conc;
+  o.f(kOscLastPeak) = peak ? 1.0 : 0.0;
+  o.f(kOscNcrit) += 1.0;
 }
 
 // OscillationAnalysis::checkCritPoint (oscillation.ipp:110-119).  The
 // window max/min are those of the live values (DENSE keeps them in a
 // multiset).  A middle index of -1 (DENSE reads contents[-1]) or an empty
 // window gives no critical point.
-__device__ __forceinline__ void osc_check(OscCell& o, const double* win, int m, int w,
-                                          double samples, const AnalysisDesc& A) {
-  const long cur = static_cast<long>(o.current);
-  const long live = static_cast<long>(o.live);
+__device__ __forceinline__ void osc_check(const OscRef& o, const double* win, int m, int w, double samples,
+                                          const AnalysisDesc& A) {
+  const long cur = static_cast<long>(o.f(kOscCurrent));
+  const long live = static_cast<long>(o.f(kOscLive));
   if (cur < 0 || live <= 0) return;
   const double mid = win[static_cast<size_t>(cur) * m];
-  long idx = static_cast<long>(o.start);
+  long idx = static_cast<long>(o.f(kOscStart));
   double hi = win[static_cast<size_t>(idx) * m], lo = hi;
   for (long q = 1; q < live; ++q) {
     idx = (idx == w - 1) ? 0 : idx + 1;
@@ -213,58 +242,60 @@ __device__ __forceinline__ void osc_check(OscCell& o, const double* win, int m, 
   else if (mid == lo) osc_add_crit(o, t, mid, false);
 }
 
-__device__ __forceinline__ double osc_dequeue(OscCell& o, const double* win, int m, int w) {
-  const long size = w;
-  long start = static_cast<long>(o.start);
-  const double popped = win[static_cast<size_t>(start) * m];
-  start = (start == size - 1) ? 0 : start + 1;
-  o.start = static_cast<double>(start);
-  DevQueue q{start, static_cast<long>(o.end), static_cast<long>(o.current), size};
-  if (2 * q.get_size() <= size) {
-    long cur = q.current + 1;
-    if (cur == size) cur = 0;
-    o.current = static_cast<double>(cur);
+// Queue::dequeue; returns nothing (the value only leaves the multiset).
+__device__ __forceinline__ void osc_dequeue(const OscRef& o, int w) {
+  long start = static_cast<long>(o.f(kOscStart));
+  start = (start == w - 1) ? 0 : start + 1;
+  o.f(kOscStart) = static_cast<double>(start);
+  if (2 * q_size(start, static_cast<long>(o.f(kOscEnd)), w) <= w) {
+    long cur = static_cast<long>(o.f(kOscCurrent)) + 1;
+    if (cur == w) cur = 0;
+    o.f(kOscCurrent) = static_cast<double>(cur);
   }
-  o.live -= 1.0;
-  return popped;
+  o.f(kOscLive) -= 1.0;
+}
+
+__device__ __forceinline__ OscRef osc_ref(double* st, const AnalysisDesc& A, int i, int cc) {
+  const size_t nm = static_cast<size_t>(A.nsp) * (A.cmax - A.cmin);
+  return OscRef{st + 2 + static_cast<size_t>(i) * (A.cmax - A.cmin) + cc, nm};
+}
+
+__device__ __forceinline__ double* osc_window(double* st, const AnalysisDesc& A, int i, int cc) {
+  const int m = A.cmax - A.cmin, w = A.range_steps + 1;
+  const size_t nm = static_cast<size_t>(A.nsp) * m;
+  return st + 2 + nm * kOscFields + static_cast<size_t>(i) * w * m + cc;
 }
 
 // OscillationAnalysis::update / get_peaks_and_troughs (oscillation.ipp:
 // 86-103, 154-160) for thread c's cell, species in observation order,
 // stopping at the first species whose window is still short.
-__device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& A,
-                                                const double* s_vals, int blk, int c,
-                                                double samples) {
+__device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& A, const double* s_vals, int blk,
+                                                int c, double samples) {
   if (c < A.cmin || c >= A.cmax) return;
   const int n = A.nsp, m = A.cmax - A.cmin, w = A.range_steps + 1;
   const int cc = c - A.cmin;
-  OscCell* cells = reinterpret_cast<OscCell*>(st + 2);
-  double* windows = st + 2 + static_cast<size_t>(n) * m * kOscCellDoubles;
   for (int i = 0; i < n; ++i) {
-    OscCell o = cells[static_cast<size_t>(i) * m + cc];
-    double* win = windows + static_cast<size_t>(i) * w * m + cc;
+    const OscRef o = osc_ref(st, A, i, cc);
+    double* win = osc_window(st, A, i, cc);
     const double added = s_vals[A.sp[i] * blk + c];
-    // enqueue
-    long end = static_cast<long>(o.end);
+    // Queue::enqueue
+    long end = static_cast<long>(o.f(kOscEnd));
     end = (end == w - 1) ? 0 : end + 1;
     win[static_cast<size_t>(end) * m] = added;
-    o.end = static_cast<double>(end);
-    o.live += 1.0;
-    DevQueue q{static_cast<long>(o.start), end, static_cast<long>(o.current), w};
-    if (2 * q.get_size() >= w) {
-      long cur = q.current + 1;
+    o.f(kOscEnd) = static_cast<double>(end);
+    o.f(kOscLive) += 1.0;
+    long start = static_cast<long>(o.f(kOscStart));
+    if (2 * q_size(start, end, w) >= w) {
+      long cur = static_cast<long>(o.f(kOscCurrent)) + 1;
       if (cur == w) cur = 0;
-      o.current = static_cast<double>(cur);
+      o.f(kOscCurrent) = static_cast<double>(cur);
     }
-    q.current = static_cast<long>(o.current);
-    if (q.get_size() == A.range_steps + 1) {
-      osc_dequeue(o, win, m, w);
-      q.start = static_cast<long>(o.start);
+    if (q_size(start, end, w) == A.range_steps + 1) {
+      osc_dequeue(o, w);
+      start = static_cast<long>(o.f(kOscStart));
     }
-    const bool stop = q.get_size() < A.range_steps / 2;
-    if (!stop) osc_check(o, win, m, w, samples, A);
-    cells[static_cast<size_t>(i) * m + cc] = o;
-    if (stop) break;
+    if (q_size(start, end, w) < A.range_steps / 2) break;
+    osc_check(o, win, m, w, samples, A);
   }
 }
 
@@ -277,34 +308,41 @@ __device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc
   if (c < A.cmin || c >= A.cmax) return;
   const int n = A.nsp, m = A.cmax - A.cmin, w = A.range_steps + 1;
   const int cc = c - A.cmin;
-  OscCell* cells = reinterpret_cast<OscCell*>(st + 2);
-  double* windows = st + 2 + static_cast<size_t>(n) * m * kOscCellDoubles;
   double samples = samples0;
   for (int i = 0; i < n; ++i) {
-    OscCell o = cells[static_cast<size_t>(i) * m + cc];
-    double* win = windows + static_cast<size_t>(i) * w * m + cc;
+    const OscRef o = osc_ref(st, A, i, cc);
+    double* win = osc_window(st, A, i, cc);
     samples = samples0;
     for (;;) {
-      DevQueue q{static_cast<long>(o.start), static_cast<long>(o.end), static_cast<long>(o.current), w};
-      if (!(q.get_size() >= (A.range_steps / 2) && o.live > 0.0)) break;
-      osc_dequeue(o, win, m, w);
+      const long size = q_size(static_cast<long>(o.f(kOscStart)), static_cast<long>(o.f(kOscEnd)), w);
+      if (!(size >= (A.range_steps / 2) && o.f(kOscLive) > 0.0)) break;
+      osc_dequeue(o, w);
       osc_check(o, win, m, w, samples, A);
       samples += 1.0;
     }
     osc_fold_last(o);
-    o.amp = ((o.peak_sum / o.num_peaks) - (o.trough_sum / o.num_troughs)) / 2;
-    o.per = o.cycle_sum / o.cycles;
-    o.avg_peak = (o.num_peaks != 0.0) ? o.peak_sum / o.num_peaks : o.peak_sum;
-    cells[static_cast<size_t>(i) * m + cc] = o;
+    const double np = o.f(kOscNumPeaks), nt = o.f(kOscNumTroughs);
+    o.f(kOscAmp) = ((o.f(kOscPeakSum) / np) - (o.f(kOscTroughSum) / nt)) / 2;
+    o.f(kOscPer) = o.f(kOscCycleSum) / o.f(kOscCycles);
+    o.f(kOscAvgPeak) = (np != 0.0) ? o.f(kOscPeakSum) / np : o.f(kOscPeakSum);
   }
   if (cc == m - 1) st[0] = samples;
 }
 
 // ---------------------------------------------------------------- kernel
-template <typename T, bool kKahan>
-__global__ void __launch_bounds__(256, 1) dense_step_kernel(const StepArgs a) {
-  extern __shared__ double s_vals[];  // [NS][blockDim] sampled state
-  __shared__ int s_S[kNS], s_D[kNS];
+
+// kThreads / kMinBlocks: 224 threads with two resident CTAs per SM (a
+// 144-register budget) for sets of up to 224 cells, 256 threads with one
+// CTA per SM above that.
+template <typename T, bool kKahan, int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const StepArgs a) {
+  // dynamic shared memory: sampled state [NS][blockDim] (doubles, only with
+  // analyses) | truncated delays [ND][blockDim] | the set's CSR lists
+  extern __shared__ double s_dyn[];
+  double* s_vals = s_dyn;
+  __shared__ int s_S[kNS], s_mask[kNS];
+  __shared__ int64_t s_roff[kNS];
+  __shared__ T s_prm[kNP];
   __shared__ int s_flags;
   __shared__ double s_samples[kMaxAnalyses];
 
@@ -316,48 +354,59 @@ __global__ void __launch_bounds__(256, 1) dense_step_kernel(const StepArgs a) {
   const int c = threadIdx.x;
   const bool active = c < n;
 
-  SetProgress pg = a.prog[set];
+  const SetProgress pg = a.prog[set];
   if ((pg.status & (kSetDropped | kSetNotRunnable)) || pg.finalized) return;
 
+  const int pstride = sd.param_stride;
   if (c < kNS) {
     s_S[c] = sd.S[c];
-    s_D[c] = sd.D[c];
+    s_mask[c] = sd.D[c] - 1;
+    s_roff[c] = sd.ring_off[c];
+  }
+  const T* P = static_cast<const T*>(a.params) + sd.param_base;
+  if (pstride == 0) {
+    for (int i = c; i < kNP; i += blk) s_prm[i] = P[i];
   }
   if (c == 0) s_flags = 0;
   double* anl = a.anl + sd.anl_base;
   if (c < a.n_analyses) s_samples[c] = anl[a.analyses[c].off];
   __syncthreads();
 
-  T* ring_base = static_cast<T*>(a.ring) + sd.ring_base;
-  T* ringp[kNS];
-  int head[kNS];
+  const int cell = active ? c : 0;
+  // parameters: the shared row of the set, or this cell's column of the
+  // set's [NP][n] block (read through L1)
+  const T* prm = pstride == 0 ? s_prm : P + cell;
+  const int ps = pstride == 0 ? 1 : n;
+  int* s_kd = reinterpret_cast<int*>(s_dyn + (a.n_analyses > 0 ? kNS * blk : 0));
+  int* s_csr = s_kd + kND * blk;
 #pragma unroll
-  for (int sp = 0; sp < kNS; ++sp) {
-    const int d = s_D[sp];
-    ringp[sp] = d > 0 ? ring_base + sd.ring_off[sp] : nullptr;
-    head[sp] = d > 0 ? static_cast<int>(pg.step % d) : 0;
-  }
+  for (int d = 0; d < kND; ++d) s_kd[d * blk + c] = static_cast<int>(prm[(kNR + d) * ps]);
 
-  T prm[kNP];
   T cur[kNS];
   T comp[kNS];
   T* state = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS);
-  const int cell = active ? c : 0;
-  {
-    const double* P = a.params + sd.cell_base * kNP;
 #pragma unroll
-    for (int i = 0; i < kNP; ++i) prm[i] = static_cast<T>(P[static_cast<size_t>(i) * n + cell]);
-#pragma unroll
-    for (int sp = 0; sp < kNS; ++sp) {
-      cur[sp] = state[static_cast<size_t>(sp) * n + cell];
-      comp[sp] = kKahan ? state[static_cast<size_t>(kNS + sp) * n + cell] : T(0);
-    }
+  for (int sp = 0; sp < kNS; ++sp) {
+    cur[sp] = state[static_cast<size_t>(sp) * n + cell];
+    comp[sp] = kKahan ? state[static_cast<size_t>(kNS + sp) * n + cell] : T(0);
   }
   const int* nbr_off = a.nbr_off + sd.nbr_base;
   const int nb0 = nbr_off[cell];
   const int nnbr = nbr_off[cell + 1] - nb0;
+  const int* nbr = a.nbr_idx + nb0;
+  if (a.csr_in_smem) {
+    // the set's neighbour ids, [edges], in shared memory
+    const int e0 = nbr_off[0], ne = nbr_off[n] - e0;
+    for (int e = c; e < ne; e += blk) s_csr[e] = a.nbr_idx[e0 + e];
+    nbr = s_csr + (nb0 - e0);
+  }
+  __syncthreads();
+
   int err = 0;
-  DeviceContext<T> ctx{cur, prm, ringp, head, s_S, s_D, a.nbr_idx + nb0, nnbr, n, cell, &err};
+  T* ring = static_cast<T*>(a.ring) + sd.ring_base;
+  int64_t step = pg.step;
+  DeviceContext<T> ctx{cur, prm, ps, s_kd + cell, blk, s_S, s_mask, s_roff, ring, static_cast<int>(step), nbr,
+                       nnbr, n, cell, &err};
 
   const T dt = static_cast<T>(a.dt);
   int chunk = pg.chunk;
@@ -365,7 +414,6 @@ __global__ void __launch_bounds__(256, 1) dense_step_kernel(const StepArgs a) {
                             ? sd.n_chunks
                             : chunk + a.chunk_count;
   double age = pg.age;
-  int64_t step = pg.step;
   bool dropped = false;
 
   for (; chunk < chunk_end; ++chunk) {
@@ -414,16 +462,19 @@ __global__ void __launch_bounds__(256, 1) dense_step_kernel(const StepArgs a) {
     for (int s = 0; s < sd.steps_per_chunk; ++s) {
       T nxt[kNS];
       if (active) {
-        T rates[kNR];
-#define REACTION(name) rates[name] = reaction<name>::active_rate(ctx);
-#include "reactions_list.hpp"
-#undef REACTION
+        // DENSE evaluates every rate, then adds rate * delta reaction by
+        // reaction (determ.cpp:58-72).  Each species' accumulator sees the
+        // same additions in the same order when each rate is folded in as
+        // soon as it is known, which keeps one rate live instead of all.
         T dsp[kNS];
 #pragma unroll
         for (int sp = 0; sp < kNS; ++sp) dsp[sp] = T(0);
-#define REACTION(name)                                                      \
-  _Pragma("unroll") for (int j = 0; j < num_deltas_##name; j++)             \
-      dsp[delta_ids_##name[j]] += rates[name] * static_cast<T>(deltas_##name[j]);
+#define REACTION(name)                                                        \
+  {                                                                           \
+    const T rate_ = reaction<name>::active_rate(ctx);                         \
+    _Pragma("unroll") for (int j = 0; j < num_deltas_##name; j++)             \
+        dsp[delta_ids_##name[j]] += rate_ * static_cast<T>(deltas_##name[j]); \
+  }
 #include "reactions_list.hpp"
 #undef REACTION
 #pragma unroll
@@ -437,18 +488,15 @@ __global__ void __launch_bounds__(256, 1) dense_step_kernel(const StepArgs a) {
             nxt[sp] = cur[sp] + dt * dsp[sp];
           }
         }
-      }
+        const int w = ctx.step + 1;
 #pragma unroll
-      for (int sp = 0; sp < kNS; ++sp) {
-        const int d = s_D[sp];
-        if (d > 0) {
-          int h = head[sp] + 1;
-          if (h == d) h = 0;
-          head[sp] = h;
-          if (active) ringp[sp][static_cast<size_t>(h) * n + c] = nxt[sp];
+        for (int sp = 0; sp < kNS; ++sp) {
+          const int m = s_mask[sp];
+          if (m >= 0) ring[s_roff[sp] + static_cast<int64_t>(w & m) * n + c] = nxt[sp];
         }
       }
       __syncthreads();
+      ctx.step += 1;
       if (active) {
 #pragma unroll
         for (int sp = 0; sp < kNS; ++sp) cur[sp] = nxt[sp];
@@ -531,14 +579,11 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
         st[i] = v;
       }
     } else if (A.kind == kOscillation) {
-      const int64_t cellsz = static_cast<int64_t>(nsp) * m * kOscCellDoubles;
-      const int64_t total = 2 + cellsz + static_cast<int64_t>(nsp) * (A.range_steps + 1) * m;
+      const int64_t nm = static_cast<int64_t>(nsp) * m;
+      const int64_t total = 2 + nm * kOscFields + static_cast<int64_t>(nsp) * (A.range_steps + 1) * m;
       for (int64_t i = threadIdx.x; i < total; i += blockDim.x) {
         double v = 0.0;
-        if (i >= 2 && i < 2 + cellsz) {
-          const int f = static_cast<int>((i - 2) % kOscCellDoubles);
-          if (f == 1 || f == 2) v = -1.0;  // end = current = -1
-        }
+        if (i >= 2 + kOscEnd * nm && i < 2 + (kOscCurrent + 1) * nm) v = -1.0;  // end = current = -1
         st[i] = v;
       }
     } else {
@@ -569,13 +614,18 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
   cudaError_t launch_step_##SUFFIX(const StepArgs& a, size_t smem, cudaStream_t s) {            \
     static bool configured = false;                                                             \
     if (!configured) {                                                                          \
-      cudaError_t e = cudaFuncSetAttribute(dense_step_kernel<T, KAHAN>,                          \
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,          \
-                                           kNS * kMaxCellsPerSet * (int)sizeof(double));         \
+      cudaError_t e = cudaFuncSetAttribute(dense_step_kernel<T, KAHAN, 224, 2>,                  \
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 100000); \
+      if (e != cudaSuccess) return e;                                                           \
+      e = cudaFuncSetAttribute(dense_step_kernel<T, KAHAN, 256, 1>,                              \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 200000);             \
       if (e != cudaSuccess) return e;                                                           \
       configured = true;                                                                        \
     }                                                                                           \
-    dense_step_kernel<T, KAHAN><<<a.num_sets, a.block_threads, smem, s>>>(a);                    \
+    if (a.block_threads <= 224)                                                                 \
+      dense_step_kernel<T, KAHAN, 224, 2><<<a.num_sets, a.block_threads, smem, s>>>(a);          \
+    else                                                                                        \
+      dense_step_kernel<T, KAHAN, 256, 1><<<a.num_sets, a.block_threads, smem, s>>>(a);          \
     return cudaGetLastError();                                                                  \
   }                                                                                             \
   }
