@@ -427,9 +427,21 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   a.interval = interval;
   a.chunk_count = -1;
   a.block_threads = std::max(32, (max_cells + 31) / 32 * 32);
+  a.uniform_params = 1;
+  for (const SetDesc& d : e->sets)
+    if (d.param_stride != 0) a.uniform_params = 0;
   // shared memory: sampled state (with analyses), truncated delays, and
   // each set's neighbour ids when the largest list fits
-  size_t smem = (a.n_analyses > 0 ? sizeof(double) * NUM_SPECIES * a.block_threads : 0) +
+  // rows of the sampled-state buffer: the species some analysis observes
+  a.n_vals = 0;
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) a.val_slot[sp] = -1;
+  for (auto& A : e->analyses)
+    for (int i = 0; i < A.nsp; ++i)
+      if (a.val_slot[A.sp[i]] < 0) a.val_slot[A.sp[i]] = a.n_vals++;
+  for (int i = 0; i < a.n_analyses; ++i)
+    for (int k = 0; k < a.analyses[i].nsp; ++k) a.analyses[i].slot[k] = a.val_slot[a.analyses[i].sp[k]];
+  e->analyses.assign(a.analyses, a.analyses + a.n_analyses);
+  size_t smem = (a.n_analyses > 0 ? sizeof(double) * a.n_vals * a.block_threads : 0) +
                 sizeof(int) * NUM_DELAY_REACTIONS * a.block_threads;
   const size_t csr_bytes = sizeof(int) * max_edges;
   const size_t smem_cap = a.block_threads <= 224 ? 100000 : 200000;

@@ -34,6 +34,7 @@ struct AnalysisDesc {
   int kind;
   int nsp;              // observed species count (ConcCheck: 1, or NS for all)
   int sp[kNS];          // observed species ids, in observation order
+  int slot[kNS];        // row of each observed species in the kernel's sampled-state buffer
   int cmin, cmax;       // cell range [cmin, cmax)
   double t0, t1;        // time range [t0, t1)
   int range_steps;      // oscillation window (range / anlys-intvl, truncated)
@@ -54,6 +55,7 @@ enum OscField : int {
   kOscTm2, kOscTm1,                 // times of critical points ncrit-3 and ncrit-2
   kOscPeakSum, kOscTroughSum, kOscNumPeaks, kOscNumTroughs, kOscCycleSum, kOscCycles,
   kOscAmp, kOscPer, kOscAvgPeak,    // results, written by finalize
+  kOscHi, kOscLo, kOscExtValid,     // window max/min while valid (1), else rescanned
   kOscFields
 };
 
@@ -100,6 +102,9 @@ struct StepArgs {
   int chunk_count;          // chunks to run in this launch (-1: to the end)
   int block_threads;
   int csr_in_smem;          // copy each set's neighbour ids into shared memory
+  int uniform_params;       // every set has one parameter row for all its cells
+  int n_vals;               // species the analyses observe (rows of the sampled-state buffer)
+  int val_slot[kNS];        // row of each species in that buffer, -1 when no analysis observes it
 };
 
 }  // namespace dense_b200

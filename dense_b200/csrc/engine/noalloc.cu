@@ -282,6 +282,7 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   NA_TRY(launch_init_fp64(a, reinterpret_cast<const double*>(base + o_conc),
                           reinterpret_cast<const int*>(base + o_status), s));
   a.csr_in_smem = 0;
+  a.uniform_params = 0;  // parameters are laid out per cell here
   NA_TRY(launch_step_fp64(a, sizeof(int) * NUM_DELAY_REACTIONS * a.block_threads, s));
 
   // ---- results to the caller's buffers

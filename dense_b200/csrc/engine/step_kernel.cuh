@@ -42,7 +42,12 @@ struct DelayArg {
   __device__ __forceinline__ operator T() const { return prm[(kNR + dr) * pstride]; }
 };
 
-template <typename T>
+// kUniform: every cell of the set has the set's parameters, so the lag of
+// each (delay reaction, species) read is the same for all cells and is
+// looked up in per-set tables (olag / nlag, [ND][NS]): a value >= 0 is a
+// lag the staging holds (own reads: 0 means the register state), -1 sends
+// the read through the checked path, which also records the error.
+template <typename T, bool kUniform>
 struct DeviceContext {
   const T* cur;            // this cell's lag-0 state [NS] (registers)
   const T* prm;            // parameters: shared row (pstride 1) or this cell's column (pstride n)
@@ -56,6 +61,8 @@ struct DeviceContext {
   int step;                // Euler steps done: lag 0 sits in row step & mask
   const int* nbr;          // this cell's neighbour ids (shared, or global for large lists)
   int nnbr;
+  const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
+  const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
   int n_cells;
   int cell;
   int* err;
@@ -77,6 +84,19 @@ struct DeviceContext {
     return ring[roff[sp] + static_cast<int64_t>((step - lag) & m) * n_cells + cell];
   }
 
+  __device__ __forceinline__ T own_lag(specie_id sp, int lag) const {
+    if (lag == 0) return cur[sp];
+    return ring[roff[sp] + static_cast<int64_t>((step - lag) & mask[sp]) * n_cells + cell];
+  }
+
+  __device__ __forceinline__ T nbr_lag(specie_id sp, int lag) const {
+    const T* row = ring + roff[sp] + static_cast<int64_t>((step - lag) & mask[sp]) * n_cells;
+    T sum = T(0);
+    for (int e = 0; e < nnbr; ++e) sum += row[nbr[e]];
+    T avg = sum / static_cast<T>(nnbr);
+    return isnan(avg) ? T(0) : avg;
+  }
+
   __device__ __forceinline__ T nbr_avg(specie_id sp, int k) const {
     const int s = S[sp];
     int lag = k;
@@ -92,11 +112,7 @@ struct DeviceContext {
       *err |= (lag == s - 1) ? kSetOrderedReads : kSetUnstagedLag;
       return T(0);
     }
-    const T* row = ring + roff[sp] + static_cast<int64_t>((step - lag) & m) * n_cells;
-    T sum = T(0);
-    for (int e = 0; e < nnbr; ++e) sum += row[nbr[e]];
-    T avg = sum / static_cast<T>(nnbr);
-    return isnan(avg) ? T(0) : avg;
+    return nbr_lag(sp, lag);
   }
 
   // Context::getCon(sp) -> get_concentration(cell, sp, 1) -> row_at(sp, 0).
@@ -104,12 +120,24 @@ struct DeviceContext {
   // Context::getCon(sp, delay) -> row_at(sp, 1 - delay)[cell]
   // (sim/base.hpp:419-422, determ.hpp:77-79): lag (k - 1) mod S.
   __device__ __forceinline__ T getCon(specie_id sp, int k) const { return own(sp, k); }
-  __device__ __forceinline__ T getCon(specie_id sp, DelayArg<T> d) const { return own(sp, d.k); }
+  __device__ __forceinline__ T getCon(specie_id sp, DelayArg<T> d) const {
+    if (kUniform) {
+      const int lag = olag[d.dr * kNS + sp];
+      if (lag >= 0) return own_lag(sp, lag);
+    }
+    return own(sp, d.k);
+  }
   // Context::calculateNeighborAvg -> calculate_neighbor_average
   // (determ.hpp:81-89): row_at(sp, -delay), lag k mod S, ascending
   // neighbour order, sum / count, NaN -> 0.
   __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, int k = 0) const { return nbr_avg(sp, k); }
-  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, DelayArg<T> d) const { return nbr_avg(sp, d.k); }
+  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, DelayArg<T> d) const {
+    if (kUniform) {
+      const int lag = nlag[d.dr * kNS + sp];
+      if (lag >= 0) return nbr_lag(sp, lag);
+    }
+    return nbr_avg(sp, d.k);
+  }
   // Context::getRate / getDelay / getCritVal (sim/base.hpp:393-412).  NaN
   // rates and delays are rejected when the batch is created.
   __device__ __forceinline__ T getRate(reaction_id r) const { return prm[r * pstride]; }
@@ -136,7 +164,7 @@ __device__ __forceinline__ void basic_cell_update(double* st, const AnalysisDesc
   double* csums = cmaxs + static_cast<size_t>(m) * n;
   const int cc = c - A.cmin;
   for (int i = 0; i < n; ++i) {
-    const double x = s_vals[A.sp[i] * blk + c];
+    const double x = s_vals[A.slot[i] * blk + c];
     const size_t k = static_cast<size_t>(i) * m + cc;
     const double mn = cmins[k], mx = cmaxs[k];
     cmins[k] = (mn < x) ? mn : x;
@@ -154,7 +182,7 @@ __device__ __forceinline__ void basic_range_fold(double* st, const AnalysisDesc&
   const int n = A.nsp;
   for (int i = lane; i < n; i += 32) {
     double mn = st[i], mx = st[n + i], sm = st[2 * n + i];
-    const double* v = s_vals + A.sp[i] * blk;
+    const double* v = s_vals + A.slot[i] * blk;
     for (int c = A.cmin; c < A.cmax; ++c) {
       const double x = v[c];
       mn = (mn < x) ? mn : x;
@@ -178,8 +206,13 @@ struct OscRef {
   __device__ __forceinline__ double& f(int k) const { return p[k * stride]; }
 };
 
-// Queue::getSize with start/end/size as DENSE computes it.
-__device__ __forceinline__ long q_size(long start, long end, long size) { return (size + end - start) % size + 1; }
+// Queue::getSize, (size + end - start) % size + 1.  With end in [-1, size)
+// and start in [0, size) the dividend lies in [0, 2 * size), so one
+// conditional subtraction gives the same remainder.
+__device__ __forceinline__ long q_size(long start, long end, long size) {
+  const long x = size + end - start;
+  return (x < size ? x : x - size) + 1;
+}
 
 __device__ __forceinline__ void osc_fold_last(const OscRef& o) {
   const double ncrit = o.f(kOscNcrit);
@@ -218,41 +251,73 @@ __device__ __forceinline__ void osc_add_crit(const OscRef& o, double t, double c
   o.f(kOscNcrit) += 1.0;
 }
 
+// The queue part of one (species, cell), held in registers while a sample
+// is processed; loaded and stored as one batch of independent accesses.
+struct OscQueue {
+  long start, end, current, live;
+  bool ext_valid;
+  double hi, lo;
+  __device__ __forceinline__ void load(const OscRef& o) {
+    const double s0 = o.f(kOscStart), e0 = o.f(kOscEnd), c0 = o.f(kOscCurrent), l0 = o.f(kOscLive);
+    const double v0 = o.f(kOscExtValid), h0 = o.f(kOscHi), w0 = o.f(kOscLo);
+    start = static_cast<long>(s0);
+    end = static_cast<long>(e0);
+    current = static_cast<long>(c0);
+    live = static_cast<long>(l0);
+    ext_valid = v0 != 0.0;
+    hi = h0;
+    lo = w0;
+  }
+  __device__ __forceinline__ void store(const OscRef& o) const {
+    o.f(kOscStart) = static_cast<double>(start);
+    o.f(kOscEnd) = static_cast<double>(end);
+    o.f(kOscCurrent) = static_cast<double>(current);
+    o.f(kOscLive) = static_cast<double>(live);
+    o.f(kOscExtValid) = ext_valid ? 1.0 : 0.0;
+    o.f(kOscHi) = hi;
+    o.f(kOscLo) = lo;
+  }
+  // Queue::dequeue.  The value leaves the multiset; if it was the window's
+  // max or min the cached extremes are dropped and the next check rescans.
+  __device__ __forceinline__ void dequeue(const double* win, int m, int w) {
+    if (ext_valid) {
+      const double v = win[static_cast<size_t>(start) * m];
+      if (v == hi || v == lo) ext_valid = false;
+    }
+    start = (start == w - 1) ? 0 : start + 1;
+    if (2 * q_size(start, end, w) <= w) {
+      current = current + 1;
+      if (current == w) current = 0;
+    }
+    live -= 1;
+  }
+};
+
 // OscillationAnalysis::checkCritPoint (oscillation.ipp:110-119).  The
 // window max/min are those of the live values (DENSE keeps them in a
 // multiset).  A middle index of -1 (DENSE reads contents[-1]) or an empty
 // window gives no critical point.
-__device__ __forceinline__ void osc_check(const OscRef& o, const double* win, int m, int w, double samples,
-                                          const AnalysisDesc& A) {
-  const long cur = static_cast<long>(o.f(kOscCurrent));
-  const long live = static_cast<long>(o.f(kOscLive));
-  if (cur < 0 || live <= 0) return;
-  const double mid = win[static_cast<size_t>(cur) * m];
-  long idx = static_cast<long>(o.f(kOscStart));
-  double hi = win[static_cast<size_t>(idx) * m], lo = hi;
-  for (long q = 1; q < live; ++q) {
-    idx = (idx == w - 1) ? 0 : idx + 1;
-    const double x = win[static_cast<size_t>(idx) * m];
-    hi = (hi < x) ? x : hi;
-    lo = (x < lo) ? x : lo;
+__device__ __forceinline__ void osc_check(const OscRef& o, OscQueue& q, const double* win, int m, int w,
+                                          double samples, const AnalysisDesc& A) {
+  if (q.current < 0 || q.live <= 0) return;
+  const double mid = win[static_cast<size_t>(q.current) * m];
+  if (!q.ext_valid) {
+    long idx = q.start;
+    double hi = win[static_cast<size_t>(idx) * m], lo = hi;
+    for (long k = 1; k < q.live; ++k) {
+      idx = (idx == w - 1) ? 0 : idx + 1;
+      const double x = win[static_cast<size_t>(idx) * m];
+      hi = (hi < x) ? x : hi;
+      lo = (x < lo) ? x : lo;
+    }
+    q.hi = hi;
+    q.lo = lo;
+    q.ext_valid = true;
   }
   double t = (samples - static_cast<double>(A.range_steps / 2)) * A.interval + A.t0;
   t = (0.0 < t) ? t : 0.0;
-  if (mid == hi && mid != lo) osc_add_crit(o, t, mid, true);
-  else if (mid == lo) osc_add_crit(o, t, mid, false);
-}
-
-// Queue::dequeue; returns nothing (the value only leaves the multiset).
-__device__ __forceinline__ void osc_dequeue(const OscRef& o, int w) {
-  long start = static_cast<long>(o.f(kOscStart));
-  start = (start == w - 1) ? 0 : start + 1;
-  o.f(kOscStart) = static_cast<double>(start);
-  if (2 * q_size(start, static_cast<long>(o.f(kOscEnd)), w) <= w) {
-    long cur = static_cast<long>(o.f(kOscCurrent)) + 1;
-    if (cur == w) cur = 0;
-    o.f(kOscCurrent) = static_cast<double>(cur);
-  }
-  o.f(kOscLive) -= 1.0;
+  if (mid == q.hi && mid != q.lo) osc_add_crit(o, t, mid, true);
+  else if (mid == q.lo) osc_add_crit(o, t, mid, false);
 }
 
 __device__ __forceinline__ OscRef osc_ref(double* st, const AnalysisDesc& A, int i, int cc) {
@@ -277,25 +342,26 @@ __device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& 
   for (int i = 0; i < n; ++i) {
     const OscRef o = osc_ref(st, A, i, cc);
     double* win = osc_window(st, A, i, cc);
-    const double added = s_vals[A.sp[i] * blk + c];
-    // Queue::enqueue
-    long end = static_cast<long>(o.f(kOscEnd));
-    end = (end == w - 1) ? 0 : end + 1;
-    win[static_cast<size_t>(end) * m] = added;
-    o.f(kOscEnd) = static_cast<double>(end);
-    o.f(kOscLive) += 1.0;
-    long start = static_cast<long>(o.f(kOscStart));
-    if (2 * q_size(start, end, w) >= w) {
-      long cur = static_cast<long>(o.f(kOscCurrent)) + 1;
-      if (cur == w) cur = 0;
-      o.f(kOscCurrent) = static_cast<double>(cur);
+    const double added = s_vals[A.slot[i] * blk + c];
+    OscQueue q;
+    q.load(o);
+    // Queue::enqueue; the multiset gains `added`
+    q.end = (q.end == w - 1) ? 0 : q.end + 1;
+    win[static_cast<size_t>(q.end) * m] = added;
+    q.live += 1;
+    if (q.ext_valid) {
+      q.hi = (q.hi < added) ? added : q.hi;
+      q.lo = (added < q.lo) ? added : q.lo;
     }
-    if (q_size(start, end, w) == A.range_steps + 1) {
-      osc_dequeue(o, w);
-      start = static_cast<long>(o.f(kOscStart));
+    if (2 * q_size(q.start, q.end, w) >= w) {
+      q.current = q.current + 1;
+      if (q.current == w) q.current = 0;
     }
-    if (q_size(start, end, w) < A.range_steps / 2) break;
-    osc_check(o, win, m, w, samples, A);
+    if (q_size(q.start, q.end, w) == A.range_steps + 1) q.dequeue(win, m, w);
+    const bool stop = q_size(q.start, q.end, w) < A.range_steps / 2;
+    if (!stop) osc_check(o, q, win, m, w, samples, A);
+    q.store(o);
+    if (stop) break;
   }
 }
 
@@ -313,13 +379,15 @@ __device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc
     const OscRef o = osc_ref(st, A, i, cc);
     double* win = osc_window(st, A, i, cc);
     samples = samples0;
+    OscQueue q;
+    q.load(o);
     for (;;) {
-      const long size = q_size(static_cast<long>(o.f(kOscStart)), static_cast<long>(o.f(kOscEnd)), w);
-      if (!(size >= (A.range_steps / 2) && o.f(kOscLive) > 0.0)) break;
-      osc_dequeue(o, w);
-      osc_check(o, win, m, w, samples, A);
+      if (!(q_size(q.start, q.end, w) >= (A.range_steps / 2) && q.live > 0)) break;
+      q.dequeue(win, m, w);
+      osc_check(o, q, win, m, w, samples, A);
       samples += 1.0;
     }
+    q.store(o);
     osc_fold_last(o);
     const double np = o.f(kOscNumPeaks), nt = o.f(kOscNumTroughs);
     o.f(kOscAmp) = ((o.f(kOscPeakSum) / np) - (o.f(kOscTroughSum) / nt)) / 2;
@@ -334,7 +402,7 @@ __device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc
 // kThreads / kMinBlocks: 224 threads with two resident CTAs per SM (a
 // 144-register budget) for sets of up to 224 cells, 256 threads with one
 // CTA per SM above that.
-template <typename T, bool kKahan, int kThreads, int kMinBlocks>
+template <typename T, bool kKahan, int kThreads, int kMinBlocks, bool kUniform>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const StepArgs a) {
   // dynamic shared memory: sampled state [NS][blockDim] (doubles, only with
   // analyses) | truncated delays [ND][blockDim] | the set's CSR lists
@@ -345,6 +413,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   __shared__ T s_prm[kNP];
   __shared__ int s_flags;
   __shared__ double s_samples[kMaxAnalyses];
+  __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
 
   const int set = blockIdx.x;
   if (set >= a.num_sets) return;
@@ -377,7 +446,24 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   // set's [NP][n] block (read through L1)
   const T* prm = pstride == 0 ? s_prm : P + cell;
   const int ps = pstride == 0 ? 1 : n;
-  int* s_kd = reinterpret_cast<int*>(s_dyn + (a.n_analyses > 0 ? kNS * blk : 0));
+  if (kUniform) {
+    // lag tables of this set, with the exact lag rules of the checked path
+    for (int i = c; i < kND * kNS; i += blk) {
+      const int d = i / kNS, sp = i % kNS;
+      const int k = static_cast<int>(s_prm[kNR + d]);
+      const int S = s_S[sp], m = s_mask[sp];
+      int ol = -1, nl = -1;
+      if (k >= 0 && k <= S) {  // else: the checked path records a bad delay
+        ol = k - 1 < 0 ? S - 1 : k - 1;
+        if (ol != 0 && ol > m) ol = -1;
+        nl = k == S ? 0 : k;
+        if (nl >= m || nl == S - 1) nl = -1;
+      }
+      s_olag[i] = ol;
+      s_nlag[i] = nl;
+    }
+  }
+  int* s_kd = reinterpret_cast<int*>(s_dyn + (a.n_analyses > 0 ? a.n_vals * blk : 0));
   int* s_csr = s_kd + kND * blk;
 #pragma unroll
   for (int d = 0; d < kND; ++d) s_kd[d * blk + c] = static_cast<int>(prm[(kNR + d) * ps]);
@@ -405,8 +491,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   int err = 0;
   T* ring = static_cast<T*>(a.ring) + sd.ring_base;
   int64_t step = pg.step;
-  DeviceContext<T> ctx{cur, prm, ps, s_kd + cell, blk, s_S, s_mask, s_roff, ring, static_cast<int>(step), nbr,
-                       nnbr, n, cell, &err};
+  DeviceContext<T, kUniform> ctx{cur,  prm,    ps,   s_kd + cell, blk,    s_S,    s_mask, s_roff, ring,
+                                 static_cast<int>(step), nbr, nnbr, s_olag, s_nlag, n, cell, &err};
 
   const T dt = static_cast<T>(a.dt);
   int chunk = pg.chunk;
@@ -420,7 +506,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
     // ---- analyses sample the state at `age` (measurement/base.ipp:4-9)
     if (a.n_analyses > 0) {
 #pragma unroll
-      for (int sp = 0; sp < kNS; ++sp) s_vals[sp * blk + c] = static_cast<double>(cur[sp]);
+      for (int sp = 0; sp < kNS; ++sp) {
+        const int row = a.val_slot[sp];
+        if (row >= 0) s_vals[row * blk + c] = static_cast<double>(cur[sp]);
+      }
       __syncthreads();
       bool bad = false;
       for (int ai = 0; ai < a.n_analyses; ++ai) {
@@ -443,7 +532,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
           if (!in_range) continue;
           if (c >= A.cmin && c < A.cmax) {
             for (int i = 0; i < A.nsp; ++i) {
-              const double x = s_vals[A.sp[i] * blk + c];
+              const double x = s_vals[A.slot[i] * blk + c];
               if (x < A.lo || x > A.hi) bad = true;
             }
           }
@@ -604,6 +693,19 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
 }  // namespace dense_b200
 
 // Launchers, named by the including translation unit's precision suffix.
+#define DENSE_B200_STEP_VARIANT(T, KAHAN, THREADS, BLOCKS, UNIFORM, SMEM_CAP)                     \
+  {                                                                                             \
+    auto k = dense_step_kernel<T, KAHAN, THREADS, BLOCKS, UNIFORM>;                             \
+    static bool configured = false;                                                             \
+    if (!configured) {                                                                          \
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP); \
+      if (e != cudaSuccess) return e;                                                           \
+      configured = true;                                                                        \
+    }                                                                                           \
+    k<<<a.num_sets, a.block_threads, smem, s>>>(a);                                             \
+    return cudaGetLastError();                                                                  \
+  }
+
 #define DENSE_B200_DEFINE_LAUNCHERS(SUFFIX, T, KAHAN)                                             \
   namespace dense_b200 {                                                                        \
   cudaError_t launch_init_##SUFFIX(const StepArgs& a, const double* init_conc,                   \
@@ -612,20 +714,12 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
     return cudaGetLastError();                                                                  \
   }                                                                                             \
   cudaError_t launch_step_##SUFFIX(const StepArgs& a, size_t smem, cudaStream_t s) {            \
-    static bool configured = false;                                                             \
-    if (!configured) {                                                                          \
-      cudaError_t e = cudaFuncSetAttribute(dense_step_kernel<T, KAHAN, 224, 2>,                  \
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 100000); \
-      if (e != cudaSuccess) return e;                                                           \
-      e = cudaFuncSetAttribute(dense_step_kernel<T, KAHAN, 256, 1>,                              \
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, 200000);             \
-      if (e != cudaSuccess) return e;                                                           \
-      configured = true;                                                                        \
+    if (a.block_threads <= 224) {                                                               \
+      if (a.uniform_params) DENSE_B200_STEP_VARIANT(T, KAHAN, 224, 2, true, 100000)              \
+      else DENSE_B200_STEP_VARIANT(T, KAHAN, 224, 2, false, 100000)                               \
+    } else {                                                                                    \
+      if (a.uniform_params) DENSE_B200_STEP_VARIANT(T, KAHAN, 256, 1, true, 200000)              \
+      else DENSE_B200_STEP_VARIANT(T, KAHAN, 256, 1, false, 200000)                               \
     }                                                                                           \
-    if (a.block_threads <= 224)                                                                 \
-      dense_step_kernel<T, KAHAN, 224, 2><<<a.num_sets, a.block_threads, smem, s>>>(a);          \
-    else                                                                                        \
-      dense_step_kernel<T, KAHAN, 256, 1><<<a.num_sets, a.block_threads, smem, s>>>(a);          \
-    return cudaGetLastError();                                                                  \
   }                                                                                             \
   }
