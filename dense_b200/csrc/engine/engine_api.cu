@@ -98,7 +98,37 @@ struct LagTracer {
 struct SetPlan {
   SetDesc d;
   int status = 0;
+  bool use_mem = false;         // run by the memory-state kernel
+  std::vector<int> lvl_off;     // memory kernel: level offsets into lvl_cells
+  std::vector<int> lvl_cells;   // memory kernel: cells in level order
 };
+
+// Cell-dependency levels of DENSE's in-order cell loop for reads of the
+// row written in the same step: level(c) = 1 + the highest level of c's
+// lower-numbered neighbours (0 without any), cells of a level in id order.
+void plan_levels(const dense_set_desc& in, bool ordered, SetPlan& plan) {
+  const int n = in.num_cells;
+  std::vector<int> level(n, 0);
+  int n_levels = 1;
+  if (ordered) {
+    for (int c = 0; c < n; ++c) {
+      int l = 0;
+      for (int k = in.nbr_offsets[c]; k < in.nbr_offsets[c + 1]; ++k) {
+        const int v = in.nbr_ids[k];
+        if (v < c) l = std::max(l, level[v] + 1);
+      }
+      level[c] = l;
+      n_levels = std::max(n_levels, l + 1);
+    }
+  }
+  plan.lvl_off.assign(n_levels + 1, 0);
+  for (int c = 0; c < n; ++c) plan.lvl_off[level[c] + 1]++;
+  for (int l = 0; l < n_levels; ++l) plan.lvl_off[l + 1] += plan.lvl_off[l];
+  plan.lvl_cells.assign(n, 0);
+  std::vector<int> fill(plan.lvl_off.begin(), plan.lvl_off.end() - 1);
+  for (int c = 0; c < n; ++c) plan.lvl_cells[fill[level[c]]++] = c;
+  plan.d.n_levels = n_levels;
+}
 
 struct DeviceBuffer {
   void* p = nullptr;
@@ -133,7 +163,8 @@ struct dense_engine {
   std::vector<AnalysisDesc> analyses;
   std::vector<int> init_status;
   DeviceBuffer d_sets, d_prog, d_params, d_nbr_off, d_nbr_idx, d_state, d_ring, d_anl, d_init_conc,
-      d_init_status;
+      d_init_status, d_lists, d_lvl_off, d_lvl_cells;
+  int n_reg = 0, n_mem = 0;  // sets run by the register / memory kernels (d_lists: reg then mem)
   std::map<int, cudaGraphExec_t> graphs;
   ~dense_engine() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
@@ -208,13 +239,19 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
 #undef REACTION
     }
   }
-  if (ordered) plan.status |= kSetOrderedReads;
   if (bad) plan.status |= kSetBadDelay;
+  // sets whose neighbour reads see the row written in the same step, and
+  // sets larger than a CTA, run in the memory-state kernel, which keeps
+  // every species in its ring (at least two rows)
+  d.ordered = ordered ? 1 : 0;
+  plan.use_mem = ordered || n > kStepThreads;
+  plan_levels(in, ordered, plan);
   int64_t off = 0;
   for (int sp = 0; sp < NUM_SPECIES; ++sp) {
     int depth = 0;
     if (own_max[sp] >= 1) depth = own_max[sp] + 1;
     if (nbr_max[sp] >= 0) depth = std::max(depth, nbr_max[sp] + 2);
+    if (plan.use_mem) depth = std::max(depth, 2);
     // a power of two, so a row is (step - lag) & (D - 1)
     d.D[sp] = depth > 0 ? next_pow2(depth) : 0;
     depth = d.D[sp];
@@ -271,7 +308,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   CUDA_TRY(cudaSetDevice(run->device));
 
   // ---- analyses
-  int min_cells = kStepThreads + 1;
+  int min_cells = kMaxCells + 1;
   for (int s = 0; s < num_sets; ++s) min_cells = std::min(min_cells, in_sets[s].num_cells);
   int64_t anl_block = 0;
   for (int ai = 0; ai < run->num_analyses; ++ai) {
@@ -325,14 +362,15 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   std::vector<int> off_all, idx_all;
   int64_t cells_total = 0, ring_total = 0;
   int max_cells = 0, max_edges = 0;
+  std::vector<int> reg_list, mem_list, lvl_off_all, lvl_cells_all;
   e->sets.resize(num_sets);
   e->init_status.resize(num_sets);
   std::vector<double> cp;
   for (int s = 0; s < num_sets; ++s) {
     const dense_set_desc& in = in_sets[s];
     const std::string where = "set " + std::to_string(s) + ": ";
-    if (in.num_cells <= 0 || in.num_cells > kStepThreads)
-      return fail(DENSE_ERR_UNSUPPORTED, where + "1..256 cells per set are supported");
+    if (in.num_cells <= 0 || in.num_cells > kMaxCells)
+      return fail(DENSE_ERR_UNSUPPORTED, where + "1.." + std::to_string(kMaxCells) + " cells per set are supported");
     if (!in.nbr_offsets || !in.nbr_ids || !in.set_params) return fail(DENSE_ERR_INVALID, where + "null input");
     if (!(in.duration >= 0.0)) return fail(DENSE_ERR_INVALID, where + "negative duration");
     const int n = in.num_cells;
@@ -372,8 +410,16 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     cells_total += n;
     ring_total += ring_elems(d);
     ring_total = (ring_total + 31) & ~int64_t(31);
-    max_cells = std::max(max_cells, n);
-    max_edges = std::max(max_edges, in.nbr_offsets[n]);
+    if (plan.use_mem) {
+      mem_list.push_back(s);
+      d.lvl_base = static_cast<int64_t>(lvl_off_all.size());
+      lvl_off_all.insert(lvl_off_all.end(), plan.lvl_off.begin(), plan.lvl_off.end());
+    } else {
+      reg_list.push_back(s);
+      max_cells = std::max(max_cells, n);
+      max_edges = std::max(max_edges, in.nbr_offsets[n]);
+    }
+    lvl_cells_all.insert(lvl_cells_all.end(), plan.lvl_cells.begin(), plan.lvl_cells.end());
     e->total_cell_steps += static_cast<int64_t>(n) * d.n_chunks * steps_per_chunk;
     e->sets[s] = d;
   }
@@ -392,6 +438,22 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   if ((rc = e->d_anl.alloc(sizeof(double) * anl_block * num_sets))) return rc;
   if ((rc = e->d_init_conc.alloc(sizeof(double) * conc_all.size()))) return rc;
   if ((rc = e->d_init_status.alloc(sizeof(int) * num_sets))) return rc;
+  if ((rc = e->d_lists.alloc(sizeof(int) * num_sets))) return rc;
+  if ((rc = e->d_lvl_off.alloc(sizeof(int) * std::max<size_t>(1, lvl_off_all.size())))) return rc;
+  if ((rc = e->d_lvl_cells.alloc(sizeof(int) * lvl_cells_all.size()))) return rc;
+  e->n_reg = static_cast<int>(reg_list.size());
+  e->n_mem = static_cast<int>(mem_list.size());
+  {
+    std::vector<int> lists(reg_list);
+    lists.insert(lists.end(), mem_list.begin(), mem_list.end());
+    CUDA_TRY(cudaMemcpyAsync(e->d_lists.p, lists.data(), sizeof(int) * num_sets, cudaMemcpyHostToDevice, e->stream));
+    if (!lvl_off_all.empty())
+      CUDA_TRY(cudaMemcpyAsync(e->d_lvl_off.p, lvl_off_all.data(), sizeof(int) * lvl_off_all.size(),
+                               cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->d_lvl_cells.p, lvl_cells_all.data(), sizeof(int) * lvl_cells_all.size(),
+                             cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+  }
   CUDA_TRY(cudaMemcpyAsync(e->d_sets.p, e->sets.data(), sizeof(SetDesc) * num_sets, cudaMemcpyHostToDevice, e->stream));
   std::vector<float> params_f;
   if (run->precision == DENSE_FP64) {
@@ -420,6 +482,8 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   a.state = e->d_state.p;
   a.ring = e->d_ring.p;
   a.anl = static_cast<double*>(e->d_anl.p);
+  a.lvl_off = static_cast<const int*>(e->d_lvl_off.p);
+  a.lvl_cells = static_cast<const int*>(e->d_lvl_cells.p);
   for (size_t i = 0; i < e->analyses.size(); ++i) a.analyses[i] = e->analyses[i];
   a.n_analyses = static_cast<int>(e->analyses.size());
   a.num_sets = num_sets;
@@ -466,13 +530,23 @@ int dense_engine_reset(dense_engine* e, void* stream) {
   return DENSE_OK;
 }
 
+static cudaError_t launch_all(dense_engine* e, const StepArgs& a, cudaStream_t s) {
+  const int* reg = static_cast<const int*>(e->d_lists.p);
+  const int* mem = reg + e->n_reg;
+  cudaError_t r = e->precision == DENSE_FP64 ? launch_step_fp64(a, reg, e->n_reg, e->smem, s)
+                                              : launch_step_fp32(a, reg, e->n_reg, e->smem, s);
+  if (r != cudaSuccess) return r;
+  return e->precision == DENSE_FP64 ? launch_step_mem_fp64(a, mem, e->n_mem, s)
+                                    : launch_step_mem_fp32(a, mem, e->n_mem, s);
+}
+
 int dense_engine_run(dense_engine* e, int num_chunks, void* stream) {
   if (!e) return fail(DENSE_ERR_INVALID, "null engine");
   CUDA_TRY(cudaSetDevice(e->device));
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : e->stream;
   StepArgs a = e->args;
   a.chunk_count = num_chunks < 0 ? -1 : num_chunks;
-  CUDA_TRY(e->precision == DENSE_FP64 ? launch_step_fp64(a, e->smem, s) : launch_step_fp32(a, e->smem, s));
+  CUDA_TRY(launch_all(e, a, s));
   return DENSE_OK;
 }
 
@@ -485,14 +559,14 @@ int dense_engine_run_graph(dense_engine* e, int num_chunks, void* stream) {
     // first use: make sure the kernel attributes are set outside capture
     StepArgs a0 = e->args;
     a0.chunk_count = 0;
-    CUDA_TRY(e->precision == DENSE_FP64 ? launch_step_fp64(a0, e->smem, s) : launch_step_fp32(a0, e->smem, s));
+    CUDA_TRY(launch_all(e, a0, s));
     cudaStream_t cap;
     CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaGraph_t g;
     CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     StepArgs a = e->args;
     a.chunk_count = num_chunks < 0 ? -1 : num_chunks;
-    cudaError_t le = e->precision == DENSE_FP64 ? launch_step_fp64(a, e->smem, cap) : launch_step_fp32(a, e->smem, cap);
+    cudaError_t le = launch_all(e, a, cap);
     cudaError_t ce = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
     CUDA_TRY(le);

@@ -15,7 +15,8 @@ constexpr int kNR = NUM_REACTIONS;
 constexpr int kND = NUM_DELAY_REACTIONS;
 constexpr int kNP = NUM_PARAMS;
 constexpr int kMaxAnalyses = 8;
-constexpr int kStepThreads = 256;  // one thread per cell, one CTA per set: at most 256 cells
+constexpr int kStepThreads = 256;  // register kernel: one thread per cell, one CTA per set
+constexpr int kMaxCells = 65536;   // memory kernel: cells per set
 
 // Per-set status bits (also the public DENSE_SET_* values).
 enum : int {
@@ -73,6 +74,9 @@ struct SetDesc {
   int S[kNS];            // DENSE ring size per species (baby_cl.cpp:10)
   int D[kNS];            // staged history depth, a power of two (0: lag-0 only, kept in registers)
   int64_t ring_off[kNS]; // offset of each staged ring inside the set's block
+  int64_t lvl_base;      // memory kernel: offset of this set's level offsets (n_levels + 1)
+  int n_levels;          // memory kernel: cell-dependency levels per step
+  int ordered;           // neighbour reads of the row written in the same step (DENSE's cell order)
 };
 
 // Mutable per-set progress, updated by the kernels.
@@ -103,6 +107,8 @@ struct StepArgs {
   int block_threads;
   int csr_in_smem;          // copy each set's neighbour ids into shared memory
   int uniform_params;       // every set has one parameter row for all its cells
+  const int* lvl_off;       // memory kernel: per set, first index of each level in lvl_cells
+  const int* lvl_cells;     // memory kernel: per set, its cells in level order
   int n_vals;               // species the analyses observe (rows of the sampled-state buffer)
   int val_slot[kNS];        // row of each species in that buffer, -1 when no analysis observes it
 };

@@ -233,6 +233,7 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   const size_t o_ring = o;     o = align256(o + sizeof(double) * (ring_total > 0 ? ring_total : 1));
   const size_t o_conc = o;     o = align256(o + sizeof(double) * NUM_SPECIES * num_sets);
   const size_t o_status = o;   o = align256(o + sizeof(int) * num_sets);
+  const size_t o_list = o;     o = align256(o + sizeof(int) * num_sets);
   if (o > kScratchBytes)
     return nfail(DENSE_ERR_SCRATCH_TOO_SMALL, "batch needs more than the 16 MiB scratch array");
   unsigned char* base = nullptr;
@@ -243,6 +244,9 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   NA_TRY(cudaMemcpyAsync(base + o_sets, desc, sizeof(SetDesc) * num_sets, cudaMemcpyHostToDevice, s));
   NA_TRY(cudaMemcpyAsync(base + o_conc, init_conc, sizeof(double) * NUM_SPECIES * num_sets, cudaMemcpyHostToDevice, s));
   NA_TRY(cudaMemcpyAsync(base + o_status, init_status, sizeof(int) * num_sets, cudaMemcpyHostToDevice, s));
+  int list[kMaxNoallocSets];
+  for (int si = 0; si < num_sets; ++si) list[si] = si;
+  NA_TRY(cudaMemcpyAsync(base + o_list, list, sizeof(int) * num_sets, cudaMemcpyHostToDevice, s));
   int64_t edge_base = 0;
   for (int si = 0; si < num_sets; ++si) {
     const dense_set_desc& in = sets[si];
@@ -283,7 +287,8 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
                           reinterpret_cast<const int*>(base + o_status), s));
   a.csr_in_smem = 0;
   a.uniform_params = 0;  // parameters are laid out per cell here
-  NA_TRY(launch_step_fp64(a, sizeof(int) * NUM_DELAY_REACTIONS * a.block_threads, s));
+  NA_TRY(launch_step_fp64(a, reinterpret_cast<const int*>(base + o_list), num_sets,
+                          sizeof(int) * NUM_DELAY_REACTIONS * a.block_threads, s));
 
   // ---- results to the caller's buffers
   size_t out_off = 0;

@@ -63,6 +63,7 @@ struct DeviceContext {
   int nnbr;
   const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
   const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
+  bool ordered;            // the set runs in cell-dependency levels (memory kernel)
   int n_cells;
   int cell;
   int* err;
@@ -105,11 +106,27 @@ struct DeviceContext {
       lag = (k % s + s) % s;
     }
     const int m = mask[sp];
-    // lag S-1 is the row other cells write in this very step (DENSE's
-    // cell-ordered loop reads new values of lower-numbered neighbours);
-    // this schedule does not run such reads
-    if (lag >= m || lag == s - 1) {
-      *err |= (lag == s - 1) ? kSetOrderedReads : kSetUnstagedLag;
+    // lag S-1 is the row DENSE's cell-ordered loop is writing in this very
+    // step: lower-numbered neighbours have their new value there already,
+    // the others (and the cell itself) still the old one.  Only a set run
+    // in cell-dependency levels, with rings deeper than S, reads it.
+    if (lag == s - 1 && s > 1) {
+      if (!ordered || m < s) {
+        *err |= kSetOrderedReads;
+        return T(0);
+      }
+      const T* fresh = ring + roff[sp] + static_cast<int64_t>((step + 1) & m) * n_cells;
+      const T* old = ring + roff[sp] + static_cast<int64_t>((step - lag) & m) * n_cells;
+      T sum = T(0);
+      for (int e = 0; e < nnbr; ++e) {
+        const int v = nbr[e];
+        sum += v < cell ? fresh[v] : old[v];
+      }
+      T avg = sum / static_cast<T>(nnbr);
+      return isnan(avg) ? T(0) : avg;
+    }
+    if (lag >= m) {
+      *err |= kSetUnstagedLag;
       return T(0);
     }
     return nbr_lag(sp, lag);
@@ -142,7 +159,8 @@ struct DeviceContext {
   // rates and delays are rejected when the batch is created.
   __device__ __forceinline__ T getRate(reaction_id r) const { return prm[r * pstride]; }
   __device__ __forceinline__ DelayArg<T> getDelay(delay_reaction_id d) const {
-    return DelayArg<T>{prm, pstride, static_cast<int>(d), kd[d * kd_stride]};
+    return DelayArg<T>{prm, pstride, static_cast<int>(d),
+                       kd ? kd[d * kd_stride] : static_cast<int>(prm[(kNR + d) * pstride])};
   }
   __device__ __forceinline__ T getCritVal(critspecie_id c) const { return prm[(kNR + kND + c) * pstride]; }
 };
@@ -154,8 +172,8 @@ struct DeviceContext {
 // BasicAnalysis::update (basic.ipp:22-36), per-cell part: thread c updates
 // its own column.  std::min(x, m) = (m < x) ? m : x, std::max(x, M) =
 // (x < M) ? M : x, NaN behaviour kept.
-__device__ __forceinline__ void basic_cell_update(double* st, const AnalysisDesc& A,
-                                                  const double* s_vals, int blk, int c) {
+template <typename Vals>
+__device__ __forceinline__ void basic_cell_update(double* st, const AnalysisDesc& A, const Vals& vals, int c) {
   const int n = A.nsp;
   const int m = A.cmax - A.cmin;
   if (c < A.cmin || c >= A.cmax) return;
@@ -164,7 +182,7 @@ __device__ __forceinline__ void basic_cell_update(double* st, const AnalysisDesc
   double* csums = cmaxs + static_cast<size_t>(m) * n;
   const int cc = c - A.cmin;
   for (int i = 0; i < n; ++i) {
-    const double x = s_vals[A.slot[i] * blk + c];
+    const double x = vals(A.slot[i], c);
     const size_t k = static_cast<size_t>(i) * m + cc;
     const double mn = cmins[k], mx = cmaxs[k];
     cmins[k] = (mn < x) ? mn : x;
@@ -177,14 +195,13 @@ __device__ __forceinline__ void basic_cell_update(double* st, const AnalysisDesc
 // cell order, as DENSE's loop does (cells outer, species inner; each
 // species' accumulator only sees its own values, so per-species folds in
 // cell order give the same results bit for bit).
-__device__ __forceinline__ void basic_range_fold(double* st, const AnalysisDesc& A,
-                                                 const double* s_vals, int blk, int lane) {
+template <typename Vals>
+__device__ __forceinline__ void basic_range_fold(double* st, const AnalysisDesc& A, const Vals& vals, int lane) {
   const int n = A.nsp;
   for (int i = lane; i < n; i += 32) {
     double mn = st[i], mx = st[n + i], sm = st[2 * n + i];
-    const double* v = s_vals + A.slot[i] * blk;
     for (int c = A.cmin; c < A.cmax; ++c) {
-      const double x = v[c];
+      const double x = vals(A.slot[i], c);
       mn = (mn < x) ? mn : x;
       mx = (x < mx) ? mx : x;
       sm = sm + x;
@@ -334,15 +351,16 @@ __device__ __forceinline__ double* osc_window(double* st, const AnalysisDesc& A,
 // OscillationAnalysis::update / get_peaks_and_troughs (oscillation.ipp:
 // 86-103, 154-160) for thread c's cell, species in observation order,
 // stopping at the first species whose window is still short.
-__device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& A, const double* s_vals, int blk,
-                                                int c, double samples) {
+template <typename Vals>
+__device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& A, const Vals& vals, int c,
+                                                double samples) {
   if (c < A.cmin || c >= A.cmax) return;
   const int n = A.nsp, m = A.cmax - A.cmin, w = A.range_steps + 1;
   const int cc = c - A.cmin;
   for (int i = 0; i < n; ++i) {
     const OscRef o = osc_ref(st, A, i, cc);
     double* win = osc_window(st, A, i, cc);
-    const double added = s_vals[A.slot[i] * blk + c];
+    const double added = vals(A.slot[i], c);
     OscQueue q;
     q.load(o);
     // Queue::enqueue; the multiset gains `added`
@@ -397,13 +415,67 @@ __device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc
   if (cc == m - 1) st[0] = samples;
 }
 
+// Where the analyses read the sampled state: the shared staging buffer of
+// the register kernel, or the lag-0 rows of the rings in the memory kernel.
+struct SmemVals {
+  const double* base;
+  int blk;
+  __device__ __forceinline__ double operator()(int slot, int cell) const { return base[slot * blk + cell]; }
+};
+
+template <typename T>
+struct RingVals {
+  T* const* rows;  // lag-0 row of each observed species (shared)
+  __device__ __forceinline__ double operator()(int slot, int cell) const {
+    return static_cast<double>(rows[slot][cell]);
+  }
+};
+
+// One analysis sample of a set at `age` (measurement/base.ipp:4-9): every
+// analysis records the time; those whose window contains it update, over
+// the cells c0, c0 + stride, ... this thread handles.  Returns whether a
+// concentration check failed for one of them.
+template <typename Vals>
+__device__ __forceinline__ bool analyses_sample(const StepArgs& a, double* anl, const Vals& vals, int tid, int c0,
+                                                int stride, int n, double age, const double* samples) {
+  bool bad = false;
+  for (int ai = 0; ai < a.n_analyses; ++ai) {
+    const AnalysisDesc& A = a.analyses[ai];
+    double* st = anl + A.off;
+    const bool in_range = !(age < A.t0 || age >= A.t1);
+    if (A.kind == kBasic) {
+      if (tid == 0) st[3 * A.nsp + 1] = age;
+      if (!in_range) continue;
+      for (int c = c0; c < n; c += stride) basic_cell_update(st, A, vals, c);
+      if (tid < 32) basic_range_fold(st, A, vals, tid);
+      if (tid == 0) st[3 * A.nsp] += 1.0;
+    } else if (A.kind == kOscillation) {
+      if (tid == 0) st[1] = age;
+      if (!in_range) continue;
+      for (int c = c0; c < n; c += stride) osc_cell_update(st, A, vals, c, samples[ai]);
+      if (tid == 0) st[0] = samples[ai] + 1.0;
+    } else if (A.kind == kConcCheck) {
+      if (tid == 0) st[0] = age;
+      if (!in_range) continue;
+      for (int c = c0; c < n; c += stride) {
+        if (c < A.cmin || c >= A.cmax) continue;
+        for (int i = 0; i < A.nsp; ++i) {
+          const double x = vals(A.slot[i], c);
+          if (x < A.lo || x > A.hi) bad = true;
+        }
+      }
+    }
+  }
+  return bad;
+}
+
 // ---------------------------------------------------------------- kernel
 
 // kThreads / kMinBlocks: 224 threads with two resident CTAs per SM (a
 // 144-register budget) for sets of up to 224 cells, 256 threads with one
 // CTA per SM above that.
 template <typename T, bool kKahan, int kThreads, int kMinBlocks, bool kUniform>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const StepArgs a) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const StepArgs a, const int* set_list) {
   // dynamic shared memory: sampled state [NS][blockDim] (doubles, only with
   // analyses) | truncated delays [ND][blockDim] | the set's CSR lists
   extern __shared__ double s_dyn[];
@@ -415,8 +487,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   __shared__ double s_samples[kMaxAnalyses];
   __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
 
-  const int set = blockIdx.x;
-  if (set >= a.num_sets) return;
+  const int set = set_list[blockIdx.x];
   const SetDesc& sd = a.sets[set];
   const int n = sd.n_cells;
   const int blk = blockDim.x;
@@ -492,7 +563,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   T* ring = static_cast<T*>(a.ring) + sd.ring_base;
   int64_t step = pg.step;
   DeviceContext<T, kUniform> ctx{cur,  prm,    ps,   s_kd + cell, blk,    s_S,    s_mask, s_roff, ring,
-                                 static_cast<int>(step), nbr, nnbr, s_olag, s_nlag, n, cell, &err};
+                                 static_cast<int>(step), nbr, nnbr, s_olag, s_nlag, false, n, cell, &err};
 
   const T dt = static_cast<T>(a.dt);
   int chunk = pg.chunk;
@@ -511,33 +582,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
         if (row >= 0) s_vals[row * blk + c] = static_cast<double>(cur[sp]);
       }
       __syncthreads();
-      bool bad = false;
-      for (int ai = 0; ai < a.n_analyses; ++ai) {
-        const AnalysisDesc& A = a.analyses[ai];
-        double* st = anl + A.off;
-        const bool in_range = !(age < A.t0 || age >= A.t1);
-        if (A.kind == kBasic) {
-          if (c == 0) st[3 * A.nsp + 1] = age;
-          if (!in_range) continue;
-          basic_cell_update(st, A, s_vals, blk, c);
-          if (c < 32) basic_range_fold(st, A, s_vals, blk, c);
-          if (c == 0) st[3 * A.nsp] += 1.0;
-        } else if (A.kind == kOscillation) {
-          if (c == 0) st[1] = age;
-          if (!in_range) continue;
-          osc_cell_update(st, A, s_vals, blk, c, s_samples[ai]);
-          if (c == 0) st[0] = s_samples[ai] + 1.0;
-        } else if (A.kind == kConcCheck) {
-          if (c == 0) st[0] = age;
-          if (!in_range) continue;
-          if (c >= A.cmin && c < A.cmax) {
-            for (int i = 0; i < A.nsp; ++i) {
-              const double x = s_vals[A.slot[i] * blk + c];
-              if (x < A.lo || x > A.hi) bad = true;
-            }
-          }
-        }
-      }
+      const bool bad = analyses_sample(a, anl, SmemVals{s_vals, blk}, c, c, n + blk, n, age, s_samples);
       if (bad) atomicOr(&s_flags, 1);
       __syncthreads();
       if (c < a.n_analyses) s_samples[c] = anl[a.analyses[c].off];
@@ -630,6 +675,182 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
 
 namespace dense_b200 {
 
+// Lag tables of one set (kUniform sets), with the lag rules of the checked
+// path: own reads (k-1) mod S, neighbour reads k mod S; -1 where the
+// checked path must run (out-of-range delay, unstaged lag, same-step row).
+template <typename T>
+__device__ __forceinline__ void fill_lag_tables(const T* s_prm, const int* s_S, const int* s_mask, int* s_olag,
+                                                int* s_nlag, int tid, int nthreads) {
+  for (int i = tid; i < kND * kNS; i += nthreads) {
+    const int d = i / kNS, sp = i % kNS;
+    const int k = static_cast<int>(s_prm[kNR + d]);
+    const int S = s_S[sp], m = s_mask[sp];
+    int ol = -1, nl = -1;
+    if (k >= 0 && k <= S) {
+      ol = k - 1 < 0 ? S - 1 : k - 1;
+      if (ol != 0 && ol > m) ol = -1;
+      nl = k == S ? 0 : k;
+      if (nl >= m || nl == S - 1) nl = -1;
+    }
+    s_olag[i] = ol;
+    s_nlag[i] = nl;
+  }
+}
+
+// The memory-state step kernel: one CTA per set, any number of cells, and
+// cell-dependency levels.  Every species lives in its ring (the lag-0 row
+// is the state); each step visits the levels in order, the cells of a level
+// in parallel (thread t takes the level's cells t, t + blockDim, ...), with
+// a barrier after each level.  A set whose neighbour reads see the row
+// written in the same step gets one level per step of its lower-numbered
+// neighbour chain (level(c) = 1 + max level of its lower-numbered
+// neighbours), which reproduces DENSE's cell-ordered loop; other sets have
+// one level holding every cell.
+template <typename T, bool kKahan, bool kUniform>
+__global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a, const int* set_list) {
+  __shared__ int s_S[kNS], s_mask[kNS];
+  __shared__ int64_t s_roff[kNS];
+  __shared__ T s_prm[kNP];
+  __shared__ int s_flags;
+  __shared__ double s_samples[kMaxAnalyses];
+  __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
+  __shared__ T* s_rows[kNS];
+
+  const int set = set_list[blockIdx.x];
+  const SetDesc& sd = a.sets[set];
+  const int n = sd.n_cells;
+  const int blk = blockDim.x;
+  const int tid = threadIdx.x;
+
+  const SetProgress pg = a.prog[set];
+  if ((pg.status & (kSetDropped | kSetNanParam)) || pg.finalized) return;
+
+  const int pstride = sd.param_stride;
+  const T* P = static_cast<const T*>(a.params) + sd.param_base;
+  if (tid < kNS) {
+    s_S[tid] = sd.S[tid];
+    s_mask[tid] = sd.D[tid] - 1;
+    s_roff[tid] = sd.ring_off[tid];
+  }
+  if (pstride == 0)
+    for (int i = tid; i < kNP; i += blk) s_prm[i] = P[i];
+  if (tid == 0) s_flags = 0;
+  double* anl = a.anl + sd.anl_base;
+  if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+  __syncthreads();
+  if (kUniform) fill_lag_tables(s_prm, s_S, s_mask, s_olag, s_nlag, tid, blk);
+  __syncthreads();
+
+  T* ring = static_cast<T*>(a.ring) + sd.ring_base;
+  T* comp_base = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS) + static_cast<int64_t>(kNS) * n;
+  const int* nbr_off = a.nbr_off + sd.nbr_base;
+  const int* lvl_off = a.lvl_off + sd.lvl_base;
+  const int* lvl_cells = a.lvl_cells + sd.cell_base;
+  const int n_levels = sd.n_levels;
+  const bool ordered = sd.ordered != 0;
+  int err = 0;
+  const T dt = static_cast<T>(a.dt);
+  int chunk = pg.chunk;
+  const int chunk_end = (a.chunk_count < 0 || sd.n_chunks - chunk < a.chunk_count)
+                            ? sd.n_chunks
+                            : chunk + a.chunk_count;
+  double age = pg.age;
+  int64_t step = pg.step;
+  bool dropped = false;
+
+  for (; chunk < chunk_end; ++chunk) {
+    if (a.n_analyses > 0) {
+      if (tid < kNS) {
+        const int row = a.val_slot[tid];
+        if (row >= 0) s_rows[row] = ring + s_roff[tid] + static_cast<int64_t>(step & s_mask[tid]) * n;
+      }
+      __syncthreads();
+      const bool bad = analyses_sample(a, anl, RingVals<T>{s_rows}, tid, tid, blk, n, age, s_samples);
+      if (bad) atomicOr(&s_flags, 1);
+      __syncthreads();
+      if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+      if (s_flags & 1) {
+        dropped = true;
+        break;
+      }
+    }
+    for (int s = 0; s < sd.steps_per_chunk; ++s) {
+      const int st32 = static_cast<int>(step);
+      for (int l = 0; l < n_levels; ++l) {
+        for (int i = lvl_off[l] + tid; i < lvl_off[l + 1]; i += blk) {
+          const int cell = lvl_cells[i];
+          T cur[kNS];
+#pragma unroll
+          for (int sp = 0; sp < kNS; ++sp)
+            cur[sp] = ring[s_roff[sp] + static_cast<int64_t>(st32 & s_mask[sp]) * n + cell];
+          const T* prm = pstride == 0 ? s_prm : P + cell;
+          const int ps = pstride == 0 ? 1 : n;
+          const int nb0 = nbr_off[cell];
+          DeviceContext<T, kUniform> ctx{cur,    prm,    ps,     nullptr, 0,      s_S,  s_mask, s_roff,
+                                         ring,   st32,   a.nbr_idx + nb0, nbr_off[cell + 1] - nb0,
+                                         s_olag, s_nlag, ordered, n,      cell,   &err};
+          T dsp[kNS];
+#pragma unroll
+          for (int sp = 0; sp < kNS; ++sp) dsp[sp] = T(0);
+#define REACTION(name)                                                        \
+  {                                                                           \
+    const T rate_ = reaction<name>::active_rate(ctx);                         \
+    _Pragma("unroll") for (int j = 0; j < num_deltas_##name; j++)             \
+        dsp[delta_ids_##name[j]] += rate_ * static_cast<T>(deltas_##name[j]); \
+  }
+#include "reactions_list.hpp"
+#undef REACTION
+#pragma unroll
+          for (int sp = 0; sp < kNS; ++sp) {
+            T nxt;
+            if (kKahan) {
+              T& cp = comp_base[static_cast<int64_t>(sp) * n + cell];
+              const T y = dt * dsp[sp] - cp;
+              const T t = cur[sp] + y;
+              cp = (t - cur[sp]) - y;
+              nxt = t;
+            } else {
+              nxt = cur[sp] + dt * dsp[sp];
+            }
+            ring[s_roff[sp] + static_cast<int64_t>((st32 + 1) & s_mask[sp]) * n + cell] = nxt;
+          }
+        }
+        __syncthreads();
+      }
+      ++step;
+    }
+    age += a.interval;
+  }
+
+  // lag-0 state to the state block (what read_state returns)
+  T* state = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS);
+  for (int i = tid; i < kNS * n; i += blk) {
+    const int sp = i / n, cell = i % n;
+    state[i] = ring[s_roff[sp] + static_cast<int64_t>(step & s_mask[sp]) * n + cell];
+  }
+  if (err) atomicOr(&s_flags, err << 1);
+  if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+  __syncthreads();
+  const int status = pg.status | (dropped ? kSetDropped : 0) | (s_flags >> 1);
+  const bool finish = !dropped && chunk >= sd.n_chunks;
+  if (finish) {
+    for (int ai = 0; ai < a.n_analyses; ++ai) {
+      const AnalysisDesc& A = a.analyses[ai];
+      if (A.kind == kOscillation)
+        for (int c = tid; c < n; c += blk) osc_cell_finalize(anl + A.off, A, c, s_samples[ai]);
+    }
+  }
+  if (tid == 0) {
+    SetProgress out = pg;
+    out.step = step;
+    out.chunk = chunk;
+    out.age = age;
+    out.status = status;
+    out.finalized = finish ? 1 : 0;
+    a.prog[set] = out;
+  }
+}
+
 // Fills every set's state, history rows and analysis state with their
 // initial values: all rows of every ring hold the initial concentrations
 // (determ.cpp:42-51, zeros when none are given), Basic minima start at
@@ -702,7 +923,7 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
       if (e != cudaSuccess) return e;                                                           \
       configured = true;                                                                        \
     }                                                                                           \
-    k<<<a.num_sets, a.block_threads, smem, s>>>(a);                                             \
+    k<<<n_sets, a.block_threads, smem, s>>>(a, set_list);                                       \
     return cudaGetLastError();                                                                  \
   }
 
@@ -713,7 +934,18 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
     dense_init_kernel<T><<<a.num_sets, 256, 0, s>>>(a, init_conc, init_status);                  \
     return cudaGetLastError();                                                                  \
   }                                                                                             \
-  cudaError_t launch_step_##SUFFIX(const StepArgs& a, size_t smem, cudaStream_t s) {            \
+  cudaError_t launch_step_mem_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets,       \
+                                       cudaStream_t s) {                                        \
+    if (n_sets <= 0) return cudaSuccess;                                                        \
+    if (a.uniform_params)                                                                       \
+      dense_step_mem_kernel<T, KAHAN, true><<<n_sets, 256, 0, s>>>(a, set_list);                 \
+    else                                                                                        \
+      dense_step_mem_kernel<T, KAHAN, false><<<n_sets, 256, 0, s>>>(a, set_list);                \
+    return cudaGetLastError();                                                                  \
+  }                                                                                             \
+  cudaError_t launch_step_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets, size_t smem, \
+                                   cudaStream_t s) {                                            \
+    if (n_sets <= 0) return cudaSuccess;                                                        \
     if (a.block_threads <= 224) {                                                               \
       if (a.uniform_params) DENSE_B200_STEP_VARIANT(T, KAHAN, 224, 2, true, 100000)              \
       else DENSE_B200_STEP_VARIANT(T, KAHAN, 224, 2, false, 100000)                               \

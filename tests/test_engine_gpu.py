@@ -13,7 +13,7 @@ from tests.helpers import load_fixture, mismatches, run_engine, run_oracle
 
 pytestmark = pytest.mark.gpu
 
-EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init"]
+EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init", "turing", "nan_test"]
 
 
 @pytest.mark.parametrize("name", EXACT_CASES)
@@ -39,12 +39,85 @@ def test_graph_replay_and_chunked_runs_match_one_launch():
     assert mismatches(full, run_engine("her_sets", graph=True, chunks_per_call=100)) == []
 
 
-@pytest.mark.parametrize("name", ["turing", "nan_test"])
-def test_same_step_neighbour_reads_are_reported(name):
-    # neighbour averages that read the row other cells write in the same
-    # step (DENSE's cell-ordered loop) are flagged, not silently run
-    got = run_engine(name)
-    assert got["status_0"] & E.SET_ORDERED_READS
+def _oracle_vs_engine(model, sets_spec, dt, interval, analyses, precision=0):
+    """Runs the same sets through the engine (one batch) and the oracle (one
+    simulation each); returns (engine results, oracle results) per set."""
+    from oracle.pyoracle import load_oracle
+    O = load_oracle(model)
+    b = E.Batch(model, [s for s, _ in sets_spec], dt, interval, analyses, precision=precision)
+    b.run()
+    b.sync()
+    out = []
+    st = b.status()
+    for i, (ps, cp) in enumerate(sets_spec):
+        sim = O.create(ps.nbr_offsets, ps.nbr_ids, cp, ps.set_params, ps.init_conc, dt)
+        for a in analyses:
+            sp = O_species_ids(O, a.species)
+            if a.kind == E.BASIC:
+                sim.add_basic(sp, a.cell_start, a.cell_end, a.time_start, a.time_end)
+            else:
+                sim.add_oscillation(sp, a.cell_start, a.cell_end, a.time_start, a.time_end, a.win_range,
+                                    a.anlys_intvl)
+        sim.run(ps.duration, interval)
+        eng = {"state": b.state(i), "status": st[i]}
+        ora = {"state": sim.state()}
+        for k, a in enumerate(analyses):
+            if a.kind == E.BASIC:
+                eng["b%d" % k], ora["b%d" % k] = b.basic(k, i), sim.basic(k)
+            else:
+                eng["o%d" % k], ora["o%d" % k] = b.oscillation(k, i), sim.oscillation(k)
+        out.append((eng, ora))
+    b.close()
+    return out
+
+
+def O_species_ids(O, names):
+    return [O.species.index(x) if isinstance(x, str) else int(x) for x in names]
+
+
+def _assert_same(pairs, analyses):
+    from tests.helpers import same
+    for eng, ora in pairs:
+        assert eng["status"] == 0
+        assert same(eng["state"], ora["state"])
+        for k, a in enumerate(analyses):
+            key = ("b%d" if a.kind == E.BASIC else "o%d") % k
+            fields = ("mins", "sums", "maxs", "samples", "time") if a.kind == E.BASIC else \
+                ("amps", "pers", "avg_peak", "ncrit", "samples", "time")
+            for f in fields:
+                assert same(eng[key][f], ora[key][f]), (key, f)
+
+
+def test_memory_kernel_large_her_sets_bitwise():
+    """Sets above one CTA of cells (300 and 1024) run in the memory-state
+    kernel, mixed in one batch with a 200-cell set of the register kernel."""
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    rng = np.random.Generator(np.random.PCG64(31))
+    base = workloads.template_params()
+    spec = []
+    for cells, width in ((200, 4), (300, 5), (1024, 8)):
+        off, ids = default_graph(cells, width)
+        cp = base[None, :] * rng.uniform(0.95, 1.05, size=(cells, base.size))
+        spec.append((E.ParameterSet(off, ids, base, cell_params=cp, duration=6.0), cp))
+    an = [E.Analysis.oscillation(["mh1", "ph1"], 0, 200, 0.0, float("inf"), 1.0, 0.1),
+          E.Analysis.basic(["mh1", "pd", "md"], 0, 200)]
+    _assert_same(_oracle_vs_engine("her_model_2014", spec, 0.01, 0.1, an), an)
+
+
+@pytest.mark.parametrize("grid", [16, 40])
+def test_turing_cell_ordered_reads_bitwise(grid):
+    """Turing's neighbour averages read the row DENSE's cell loop is writing
+    (lower-numbered neighbours already updated): the memory kernel's level
+    schedule must reproduce that order exactly, also on grids past one CTA."""
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    p = workloads.template_params("turing")
+    ic = np.array(workloads.templates()["turing"]["init_conc"])
+    off, ids = default_graph(grid * grid, grid)
+    spec = [(E.ParameterSet(off, ids, p, init_conc=ic, duration=3.0), np.tile(p, (grid * grid, 1)))]
+    an = [E.Analysis.basic([0, 1, 2, 3], 0, grid * grid)]
+    _assert_same(_oracle_vs_engine("turing", spec, 0.01, 0.1, an), an)
 
 
 def test_fp32_kahan_error_vs_fp64():
