@@ -92,5 +92,26 @@ def build_model(model, force=False, verbose=False):
     return out
 
 
+def cli_path(model):
+    return os.path.join(LIB_DIR, "dense_simulation_%s" % model)
+
+
+def build_cli(model, force=False):
+    """DENSE's `simulation` command for the model, linked to its engine
+    library (csrc/cli/simulation_main.cpp)."""
+    lib = build_model(model, force)
+    out = cli_path(model)
+    src = os.path.join(CSRC, "cli", "simulation_main.cpp")
+    if not force and _up_to_date(out, [src, lib, os.path.join(INCLUDE, "dense_b200.h")]):
+        return out
+    _run(["g++", "-O2", "-std=c++17", "-I", INCLUDE, src, "-o", out, "-L", LIB_DIR,
+          "-l:" + os.path.basename(lib), "-Wl,-rpath,$ORIGIN"])
+    return out
+
+
 def build_all(models=None, force=False):
-    return {m: build_model(m, force) for m in (models or MODEL_DIRS)}
+    out = {}
+    for m in (models or MODEL_DIRS):
+        out[m] = build_model(m, force)
+        build_cli(m, force)
+    return out

@@ -350,6 +350,13 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       A.lo = in.lower;
       A.hi = in.upper;
       anl_block += 1;
+    } else if (in.kind == DENSE_ANALYSIS_TRAJECTORY) {
+      // room for every sample of the longest horizon in the batch
+      int cap = 0;
+      for (int s = 0; s < num_sets; ++s)
+        cap = std::max(cap, static_cast<int>(std::ceil(in_sets[s].duration / interval)));
+      A.range_steps = cap;
+      anl_block += 2 + cap + static_cast<int64_t>(cap) * A.nsp * m;
     } else {
       return fail(DENSE_ERR_INVALID, "unknown analysis kind");
     }
@@ -444,6 +451,14 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   e->n_reg = static_cast<int>(reg_list.size());
   e->n_mem = static_cast<int>(mem_list.size());
   {
+    // longest sets first (cells x Euler steps): CTAs start in list order, so
+    // uneven horizons finish close together (longest-processing-time order)
+    auto cost = [&](int i) {
+      return static_cast<int64_t>(e->sets[i].n_cells) * e->sets[i].n_chunks * e->sets[i].steps_per_chunk;
+    };
+    auto by_cost = [&](int x, int y) { return cost(x) != cost(y) ? cost(x) > cost(y) : x < y; };
+    std::stable_sort(reg_list.begin(), reg_list.end(), by_cost);
+    std::stable_sort(mem_list.begin(), mem_list.end(), by_cost);
     std::vector<int> lists(reg_list);
     lists.insert(lists.end(), mem_list.begin(), mem_list.end());
     CUDA_TRY(cudaMemcpyAsync(e->d_lists.p, lists.data(), sizeof(int) * num_sets, cudaMemcpyHostToDevice, e->stream));
@@ -699,6 +714,27 @@ int dense_engine_read_oscillation(dense_engine* e, int analysis, int set, double
   }
   if (samples) *samples = static_cast<int>(b[0]);
   if (time) *time = b[1];
+  return DENSE_OK;
+}
+
+int dense_engine_read_trajectory(dense_engine* e, int analysis, int set, double* times, double* values,
+                                 int capacity, int* samples) {
+  if (!e || set < 0 || set >= e->num_sets || analysis < 0 || analysis >= static_cast<int>(e->analyses.size()))
+    return fail(DENSE_ERR_INVALID, "bad analysis or set index");
+  const AnalysisDesc& A = e->analyses[analysis];
+  if (A.kind != kTrajectory) return fail(DENSE_ERR_INVALID, "analysis kind mismatch");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  const double* st = static_cast<const double*>(e->d_anl.p) + e->sets[set].anl_base + A.off;
+  double cnt = 0;
+  CUDA_TRY(cudaMemcpy(&cnt, st, sizeof(double), cudaMemcpyDeviceToHost));
+  const int k = std::min(static_cast<int>(cnt), A.range_steps);
+  if (samples) *samples = k;
+  const int n = std::min(k, capacity);
+  const size_t per = static_cast<size_t>(A.nsp) * (A.cmax - A.cmin);
+  if (n > 0 && times) CUDA_TRY(cudaMemcpy(times, st + 2, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (n > 0 && values)
+    CUDA_TRY(cudaMemcpy(values, st + 2 + A.range_steps, sizeof(double) * per * n, cudaMemcpyDeviceToHost));
   return DENSE_OK;
 }
 

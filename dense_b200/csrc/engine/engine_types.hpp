@@ -28,7 +28,7 @@ enum : int {
   kSetNotRunnable = kSetNanParam | kSetOrderedReads,
 };
 
-enum AnalysisKind : int { kBasic = 1, kOscillation = 2, kConcCheck = 3 };
+enum AnalysisKind : int { kBasic = 1, kOscillation = 2, kConcCheck = 3, kTrajectory = 4 };
 
 // One analysis, identical for every set of the batch.
 struct AnalysisDesc {
@@ -49,6 +49,7 @@ struct AnalysisDesc {
 //  Basic:       mins[n] maxs[n] sums[n] samples time | cmins[n][m] cmaxs[n][m] csums[n][m]
 //  Oscillation: samples time | field[kOscFields][n][m] | window[n][w][m]
 //  ConcCheck:   time
+//  Trajectory:  samples time | sample_time[cap] | values[cap][n][m]  (cap = range_steps)
 enum OscField : int {
   kOscStart, kOscEnd, kOscCurrent,  // queue indices (core/queue.hpp)
   kOscLive,                         // values in the window

@@ -454,6 +454,22 @@ __device__ __forceinline__ bool analyses_sample(const StepArgs& a, double* anl, 
       if (!in_range) continue;
       for (int c = c0; c < n; c += stride) osc_cell_update(st, A, vals, c, samples[ai]);
       if (tid == 0) st[0] = samples[ai] + 1.0;
+    } else if (A.kind == kTrajectory) {
+      // csvw_sim::update (io/csvw_sim.ipp:17-91): every observed species
+      // of every analysed cell at every sample
+      if (tid == 0) st[1] = age;
+      if (!in_range) continue;
+      const long k = static_cast<long>(st[0]);
+      if (k < A.range_steps) {
+        const int m = A.cmax - A.cmin;
+        double* vals_k = st + 2 + A.range_steps + static_cast<size_t>(k) * A.nsp * m;
+        for (int c = c0; c < n; c += stride) {
+          if (c < A.cmin || c >= A.cmax) continue;
+          for (int i = 0; i < A.nsp; ++i) vals_k[static_cast<size_t>(i) * m + (c - A.cmin)] = vals(A.slot[i], c);
+        }
+        if (tid == 0) st[2 + k] = age;
+      }
+      if (tid == 0) st[0] = static_cast<double>(k + 1);
     } else if (A.kind == kConcCheck) {
       if (tid == 0) st[0] = age;
       if (!in_range) continue;
@@ -896,6 +912,8 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
         if (i >= 2 + kOscEnd * nm && i < 2 + (kOscCurrent + 1) * nm) v = -1.0;  // end = current = -1
         st[i] = v;
       }
+    } else if (A.kind == kTrajectory) {
+      if (threadIdx.x < 2) st[threadIdx.x] = 0.0;
     } else {
       if (threadIdx.x == 0) st[0] = 0.0;
     }

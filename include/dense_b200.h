@@ -70,6 +70,7 @@ extern "C" {
 #define DENSE_ANALYSIS_BASIC 1        /* BasicAnalysis (measurement/basic.hpp) */
 #define DENSE_ANALYSIS_OSCILLATION 2  /* OscillationAnalysis (measurement/oscillation.hpp) */
 #define DENSE_ANALYSIS_CONCCHECK 3    /* ConcentrationCheck (measurement/conccheck.hpp) */
+#define DENSE_ANALYSIS_TRAJECTORY 4   /* csvw_sim data export (io/csvw_sim.ipp) */
 
 typedef struct dense_model_info {
   int num_species;
@@ -161,6 +162,13 @@ DENSE_API int dense_engine_read_basic(dense_engine* e, int analysis, int set, do
 DENSE_API int dense_engine_read_oscillation(dense_engine* e, int analysis, int set, double* amps,
                                   double* periods, double* avg_peaks, int* num_crit, int* samples,
                                   double* time);
+
+/* Trajectory analysis `analysis` of one set: sample times [capacity] and
+   values [capacity][n][cells] of the observed species at every sample, as
+   csvw_sim::update writes them (io/csvw_sim.ipp:17-91); *samples is the
+   number recorded. */
+DENSE_API int dense_engine_read_trajectory(dense_engine* e, int analysis, int set, double* times, double* values,
+                                           int capacity, int* samples);
 
 /* Batch facts: cell-steps per full run, device bytes held, history depths. */
 DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int64_t* device_bytes,

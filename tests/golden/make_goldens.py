@@ -5,7 +5,10 @@
    (test/her_model_2014/{anlys_basic_a,anlys_oscil,cell_width_test_anlys,
    total_time_test_anlys,total_time_test_01_anlys}.csv and
    test/Nan_Test/anlys_basic_a.csv).
-2. ``ref_<case>.npz``: full-precision outputs of DENSE itself (compiled from
+2. ``inputs/`` and ``cli/<case>/``: DENSE's own ``simulation`` command
+   (oracle/_ref/<model>_simulation) run on CLI_CASES, its input files and
+   the output files it wrote.
+3. ``ref_<case>.npz``: full-precision outputs of DENSE itself (compiled from
    its sources into oracle/_ref/ by oracle/build.py and driven through
    oracle/ref_harness.cpp) on the small cases of CASES below, together with
    the inputs they were computed from.  The GPU tests compare the engine
@@ -35,6 +38,66 @@ CTEST = {
     "her_total_time_test_01_anlys.csv": "test/her_model_2014/total_time_test_01_anlys.csv",
     "nan_anlys_basic_a.csv": "test/Nan_Test/anlys_basic_a.csv",
 }
+
+
+# Input files of the command-line cases, copied as data.
+INPUTS = {
+    "her_param_sets.csv": "test/her_model_2014/param_sets.csv",
+    "her_analyses.xml": "test/her_model_2014/analyses.xml",
+    "nan_param_sets.csv": "test/Nan_Test/param_sets.csv",
+    "nan_analyses.xml": "test/Nan_Test/analyses.xml",
+    "turing_param_sets.csv": "models/Turing-Pattern/param_sets.csv",
+    "turing_init_conc.csv": "models/Turing-Pattern/init_conc.csv",
+    "organic2.graphml": "models/Turing-Pattern/organic2.graphml",
+    "cell_adj.g": "models/Turing-Pattern/cell_adj.g",
+}
+
+# DENSE's own `simulation` command (oracle/_ref/<model>_simulation) on these
+# arguments writes the expected files; {in} is the inputs directory.
+CLI_CASES = {
+    "her_test": ("her_model_2014",
+                 "-p {in}/her_param_sets.csv --cell-total 10 --tissue-width 5 --time-total 3000 --anlys-intvl .01 "
+                 "--step-size .01 --analysis {in}/her_analyses.xml", ["anlys_basic_a.csv", "anlys_oscil.csv"]),
+    "nan_test": ("nan_test",
+                 "--param-sets {in}/nan_param_sets.csv --cell-total 100 --tissue-width 100 --time-total 15 "
+                 "--anlys-intvl 0.5 -s 0.01 --analysis {in}/nan_analyses.xml", ["anlys_basic_a.csv"]),
+    "turing_graphml_export": ("turing",
+                              "-p {in}/turing_param_sets.csv -f {in}/organic2.graphml -t 4 -u 0.5 -s 0.01 "
+                              "-d {in}/turing_init_conc.csv -e traj.csv -v", ["traj.csv"]),
+    "her_edge_list_export": ("her_model_2014",
+                             "-p {in}/her_param_sets.csv -f {in}/cell_adj.g -t 30 -u 1 -s 0.01 -e traj.csv "
+                             "-o \"mh1, ph1\"", ["traj.csv"]),
+}
+
+
+def copy_inputs():
+    out = os.path.join(HERE, "inputs")
+    os.makedirs(out, exist_ok=True)
+    for dst, src in INPUTS.items():
+        shutil.copyfile(os.path.join(dense_dir(), src), os.path.join(out, dst))
+
+
+def run_cli_cases():
+    import shlex
+    import subprocess
+    import tempfile
+    from oracle.build import build_ref, ref_cli_path
+    inputs = os.path.join(HERE, "inputs")
+    for name, (model, args, outs) in CLI_CASES.items():
+        build_ref(model)
+        exe = ref_cli_path(model)
+        dst = os.path.join(HERE, "cli", name)
+        os.makedirs(dst, exist_ok=True)
+        with tempfile.TemporaryDirectory() as tmp:
+            cmd = [exe] + shlex.split(args.format(**{"in": inputs}))
+            r = subprocess.run(cmd, cwd=tmp, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            # DENSE aborts at exit ("free(): invalid pointer") after a run on
+            # an edge-list tissue; its output files are complete by then
+            if r.returncode != 0 and not all(os.path.exists(os.path.join(tmp, f)) for f in outs):
+                raise RuntimeError("DENSE failed on %s" % name)
+            for f in outs:
+                shutil.copyfile(os.path.join(tmp, f), os.path.join(dst, f))
+        print("cli", name, outs)
 
 
 def copy_ctest():
@@ -81,5 +144,7 @@ def run_ref(name):
 
 if __name__ == "__main__":
     copy_ctest()
+    copy_inputs()
+    run_cli_cases()
     for name in (sys.argv[1:] or list(CASES)):
         run_ref(name)
