@@ -202,3 +202,21 @@ def test_uneven_horizons_in_one_batch():
         assert ch[i] == n == math.ceil(durs[i] / 0.1)
         assert age[i] == sim.age()
         assert np.array_equal(b.state(i), sim.state())
+
+
+@pytest.mark.parametrize("model", ["delay_reaction", "bz", "briggs_rauscher", "nan_test", "turing"])
+def test_other_models_bitwise_vs_oracle(model):
+    """DENSE's other example models, compiled unchanged through the model
+    headers, against the oracle: random positive parameters, 24 cells,
+    initial concentrations in [0, 5)."""
+    from dense_b200.tissue import default_graph
+    L = E.load(model)
+    rng = np.random.Generator(np.random.PCG64(sum(model.encode())))
+    p = rng.uniform(0.05, 2.0, size=L.num_params)
+    if L.num_delay_reactions:
+        p[L.num_reactions:L.num_reactions + L.num_delay_reactions] = rng.uniform(0.5, 4.0, L.num_delay_reactions)
+    off, ids = default_graph(24, 6)
+    ic = rng.uniform(0.0, 5.0, size=L.num_species)
+    spec = [(E.ParameterSet(off, ids, p, init_conc=ic, duration=4.0), np.tile(p, (24, 1)))]
+    an = [E.Analysis.basic(list(range(L.num_species)), 0, 24)]
+    _assert_same(_oracle_vs_engine(model, spec, 0.01, 0.1, an), an)
