@@ -124,3 +124,154 @@ class Kernels:
         e = int(self.err.item())
         if e:
             raise RuntimeError("tensor-core GEMM reported error bits %d" % e)
+
+
+class MLP:
+    """in -> 3 x 256 GELU -> out on the tensor-core kernels.
+
+    Weights are kept as FP32 masters [out][in] with Adam moments; every step
+    casts them to BF16 (and transposed BF16 copies for the input-gradient
+    products).  Inputs are padded to IN_PAD features and outputs to OUT_PAD
+    rows (the padding weights stay zero: their gradients are zero).
+    """
+
+    def __init__(self, n_in, n_out, seed=0, device=0, lr=1e-3):
+        import torch
+        assert n_in <= IN_PAD and n_out <= OUT_PAD
+        self.torch = torch
+        self.k = Kernels(device)
+        self.dev = self.k.dev
+        self.n_in, self.n_out, self.lr = n_in, n_out, lr
+        rng = np.random.Generator(np.random.PCG64(seed))
+        shapes = [(HIDDEN, IN_PAD), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (OUT_PAD, HIDDEN)]
+        fan_in = [n_in, HIDDEN, HIDDEN, HIDDEN]
+        self.W, self.b = [], []
+        for i, (o, n) in enumerate(shapes):
+            w = np.zeros((o, n), np.float32)
+            rows = o if i < 3 else n_out
+            cols = n if i > 0 else n_in
+            w[:rows, :cols] = rng.normal(0.0, np.sqrt(2.0 / fan_in[i]), size=(rows, cols))
+            self.W.append(torch.tensor(w, device=self.dev))
+            self.b.append(torch.zeros(o, device=self.dev))
+        self.mW = [torch.zeros_like(w) for w in self.W]
+        self.vW = [torch.zeros_like(w) for w in self.W]
+        self.mb = [torch.zeros_like(b) for b in self.b]
+        self.vb = [torch.zeros_like(b) for b in self.b]
+        self.steps = 0
+        self._bufs = {}
+
+    def _buf(self, name, shape, dtype=None):
+        t = self._bufs.get(name)
+        dtype = dtype or self.torch.float32
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = self.torch.empty(shape, dtype=dtype, device=self.dev)
+            self._bufs[name] = t
+        return t
+
+    def _cast_weights(self):
+        bf = self.torch.bfloat16
+        self.Wb = [self._buf("Wb%d" % i, w.shape, bf) for i, w in enumerate(self.W)]
+        self.WTb = [self._buf("WTb%d" % i, (w.shape[1], w.shape[0]), bf) for i, w in enumerate(self.W)]
+        for i, w in enumerate(self.W):
+            self.k.cast(w, self.Wb[i])
+            if i > 0:
+                self.k.cast(w, self.WTb[i], transpose=True)
+
+    def _input(self, X):
+        """[B][n_in] float -> padded BF16 [Bp][IN_PAD], Bp a multiple of 128."""
+        B = X.shape[0]
+        Bp = (B + 127) // 128 * 128
+        Xb = self._buf("Xb", (Bp, IN_PAD), self.torch.bfloat16)
+        Xb.zero_()
+        Xb[:B, :self.n_in] = self.torch.as_tensor(X, device=self.dev, dtype=self.torch.float32).to(self.torch.bfloat16)
+        return Xb, Bp
+
+    def forward(self, Xb):
+        Bp = Xb.shape[0]
+        bf = self.torch.bfloat16
+        self.Z = [self._buf("Z%d" % i, (Bp, HIDDEN)) for i in range(3)]
+        self.H = [Xb] + [self._buf("H%d" % i, (Bp, HIDDEN), bf) for i in range(1, 4)]
+        for i in range(3):
+            self.k.gemm(self.H[i], self.Wb[i], self.Z[i], EPI_BIAS_GELU, self.b[i], self.H[i + 1])
+        Y = self._buf("Y", (Bp, OUT_PAD))
+        self.k.gemm(self.H[3], self.Wb[3], Y, EPI_BIAS, self.b[3])
+        return Y
+
+    def predict(self, X, batch=65536):
+        """Outputs [B][n_out] (float32, on the host)."""
+        self._cast_weights()
+        out = []
+        for s in range(0, X.shape[0], batch):
+            Xb, _ = self._input(X[s:s + batch])
+            Y = self.forward(Xb)
+            out.append(Y[:min(batch, X.shape[0] - s), :self.n_out].float().cpu().numpy())
+        self.k.check()
+        return np.concatenate(out) if out else np.zeros((0, self.n_out), np.float32)
+
+    def gradients(self, X, T, mask):
+        """Loss and gradients (dW, db lists) of one batch; Bp rows, padding masked."""
+        torch = self.torch
+        bf = torch.bfloat16
+        self._cast_weights()
+        Xb, Bp = self._input(X)
+        B = X.shape[0]
+        Tt = torch.zeros((Bp, self.n_out), device=self.dev)
+        Mt = torch.zeros((Bp, self.n_out), device=self.dev)
+        Tt[:B] = torch.as_tensor(np.nan_to_num(T), device=self.dev, dtype=torch.float32)
+        Mt[:B] = torch.as_tensor(mask, device=self.dev, dtype=torch.float32)
+        Y = self.forward(Xb)
+        loss = torch.zeros(1, device=self.dev)
+        dY = self._buf("dY", (Bp, OUT_PAD))
+        dYb = self._buf("dYb", (Bp, OUT_PAD), bf)
+        self.k.mse(Y, Tt, Mt, dY, dYb, loss)
+        dW = [None] * 4
+        db = [None] * 4
+        dZ, dZb = dY, dYb
+        for i in (3, 2, 1, 0):
+            rows = self.W[i].shape[0]
+            # weight gradient: dW_i = dZ^T H_i  (M = out rows, N = in, K = batch)
+            dZT = self._buf("dZT%d" % i, (rows, Bp), bf)
+            HT = self._buf("HT%d" % i, (self.W[i].shape[1], Bp), bf)
+            self.k.transpose(dZb, dZT)
+            self.k.transpose(self.H[i], HT)
+            dW[i] = self._buf("dW%d" % i, self.W[i].shape)
+            self.k.gemm(dZT, HT, dW[i])
+            db[i] = self._buf("db%d" % i, (rows,))
+            self.k.colsum(dZ, db[i])
+            if i == 0:
+                break
+            # input gradient: dH_i = dZ W_i, then dZ_{i-1} = dH_i * GELU'(Z_{i-1})
+            dH = self._buf("dH%d" % i, (Bp, HIDDEN))
+            self.k.gemm(dZb, self.WTb[i], dH)
+            ndZ = self._buf("dZ%d" % (i - 1), (Bp, HIDDEN))
+            ndZb = self._buf("dZb%d" % (i - 1), (Bp, HIDDEN), bf)
+            self.k.gelu_backward(dH, self.Z[i - 1], ndZ, ndZb)
+            dZ, dZb = ndZ, ndZb
+        self.k.check()
+        return float(loss.item()), dW, db
+
+    def step(self, X, T, mask):
+        loss, dW, db = self.gradients(X, T, mask)
+        self.steps += 1
+        for i in range(4):
+            self.k.adam(self.W[i], dW[i], self.mW[i], self.vW[i], self.lr, self.steps)
+            self.k.adam(self.b[i], db[i], self.mb[i], self.vb[i], self.lr, self.steps)
+        return loss
+
+    def fit(self, X, T, mask, epochs=20, batch=4096, seed=0, log=None):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        n = X.shape[0]
+        hist = []
+        for ep in range(epochs):
+            order = rng.permutation(n)
+            tot = 0.0
+            for s in range(0, n - batch + 1, batch):
+                idx = order[s:s + batch]
+                tot += self.step(X[idx], T[idx], mask[idx])
+            hist.append(tot / max(1, n // batch))
+            if log:
+                log("epoch %d loss %.5f" % (ep, hist[-1]))
+        return hist
+
+    def state(self):
+        return {"W": [w.cpu().numpy() for w in self.W], "b": [b.cpu().numpy() for b in self.b]}
