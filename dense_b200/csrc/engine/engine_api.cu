@@ -351,10 +351,15 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       A.hi = in.upper;
       anl_block += 1;
     } else if (in.kind == DENSE_ANALYSIS_TRAJECTORY) {
-      // room for every sample of the longest horizon in the batch
+      // room for every sample inside [time_start, time_end) of the longest
+      // horizon in the batch
       int cap = 0;
-      for (int s = 0; s < num_sets; ++s)
-        cap = std::max(cap, static_cast<int>(std::ceil(in_sets[s].duration / interval)));
+      for (int s = 0; s < num_sets; ++s) {
+        const double t1 = std::min(in.time_end, in_sets[s].duration), t0 = std::max(in.time_start, 0.0);
+        const int all = static_cast<int>(std::ceil(in_sets[s].duration / interval));
+        const int in_window = t1 > t0 ? static_cast<int>(std::ceil((t1 - t0) / interval)) + 2 : 0;
+        cap = std::max(cap, std::min(all, in_window));
+      }
       A.range_steps = cap;
       anl_block += 2 + cap + static_cast<int64_t>(cap) * A.nsp * m;
     } else {

@@ -21,6 +21,7 @@ FP32_KAHAN = 1
 BASIC = 1
 OSCILLATION = 2
 CONCCHECK = 3
+TRAJECTORY = 4
 
 SET_DROPPED = 1
 SET_NAN_PARAM = 2
@@ -69,6 +70,7 @@ _FUNCS = {
     "dense_engine_read_state": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "dense_engine_read_basic": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _I, _D]),
     "dense_engine_read_oscillation": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, _D, _I, _I, _D]),
+    "dense_engine_read_trajectory": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, C.c_int, _I]),
     "dense_engine_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _I]),
     "dense_engine_ring_info": (C.c_int, [C.c_void_p, C.c_int, _I, _I]),
     "dense_engine_destroy": (C.c_int, [C.c_void_p]),
@@ -161,6 +163,11 @@ class Analysis:
     @staticmethod
     def conccheck(species, cell_start, cell_end, lower, upper, time_start=0.0, time_end=float("inf")):
         return Analysis(CONCCHECK, species, cell_start, cell_end, time_start, time_end, lower=lower, upper=upper)
+
+    @staticmethod
+    def trajectory(species, cell_start, cell_end, time_start=0.0, time_end=float("inf")):
+        """Every sample of the observed species (csvw_sim's data export)."""
+        return Analysis(TRAJECTORY, species, cell_start, cell_end, time_start, time_end)
 
 
 def _dp(a):
@@ -273,6 +280,18 @@ class Batch:
                                                                _dp(peaks), _ip(ncrit), C.byref(samples),
                                                                C.byref(time)))
         return dict(amps=amps, pers=pers, avg_peak=peaks, ncrit=ncrit, samples=samples.value, time=time.value)
+
+    def trajectory(self, analysis, set_index):
+        """Sample times [k] and values [k][species][cells] recorded so far."""
+        a = self.analyses[analysis]
+        n, m = len(a.species), a.cell_end - a.cell_start
+        k = C.c_int()
+        self.L._check(self.L.lib.dense_engine_read_trajectory(self.h, analysis, set_index, None, None, 0, C.byref(k)))
+        times = np.zeros(k.value)
+        vals = np.zeros((k.value, n, m))
+        self.L._check(self.L.lib.dense_engine_read_trajectory(self.h, analysis, set_index, _dp(times), _dp(vals),
+                                                              k.value, C.byref(k)))
+        return times, vals
 
     def info(self):
         cs = C.c_int64()

@@ -1,0 +1,268 @@
+"""Parameter search for her_model_2014 on the batched FP64 engine, with the
+MLP surrogate in front of the simulator.
+
+DENSE's search (search/sres.hpp:202-265, sres.cpp:328-349) evolves a
+population with SRES and scores each candidate by simulating it.  Here a
+whole population is simulated as one engine batch, and the surrogate
+(dense_b200.surrogate) ranks candidates before any simulation: only the
+candidates it ranks best are simulated, and only the FP64 engine's
+results decide acceptance.
+
+Features of one simulated set (200 cells by default), all over the first
+`window` minutes -- the window of DENSE's own oscillation test
+(test/her_model_2014/analyses.xml).  DENSE passes delays in minutes where
+its history expects steps (sim/base.hpp:406-422), so the effective delays
+are ~100x shorter than the parameters say and the her clock is a transient
+that settles within ~100 simulated minutes; later windows show no
+oscillation:
+  * period    -- mean over cells of mh1's OscillationAnalysis period;
+  * amplitude -- mean over cells of mh1's OscillationAnalysis amplitude;
+  * synchrony -- mean pairwise Pearson correlation of mh1 across cells
+                 (DENSE has no synchrony measure;
+                 CorrelationAnalysis::pearson_correlate is declared but never
+                 defined, measurement/oscillation.hpp:119-136);
+  * oscillates -- finite period and amplitude above OSC_AMP.
+A candidate is accepted when its period is TARGET_PERIOD +- PERIOD_TOL and
+its amplitude at least AMP_MIN (fixed here at 50, about twice the
+template's amplitude).
+"""
+
+import math
+import time
+
+import numpy as np
+
+from . import engine as E
+from . import workloads
+from .tissue import default_graph
+
+TARGET_PERIOD = 30.0
+PERIOD_TOL = 3.0
+AMP_MIN = 50.0
+OSC_AMP = 1.0
+SPREAD = 4.0
+
+
+def template():
+    return workloads.template_params("her_model_2014")
+
+
+def active_params():
+    """Indices of the template's non-zero parameters (the search space)."""
+    return np.nonzero(template())[0]
+
+
+def draw_candidates(n, seed, spread=SPREAD):
+    """Log-uniform +-spread x around the template, [n][NP]."""
+    return workloads.log_uniform_params(n, 1.0 / spread, spread, seed=seed)
+
+
+def encode(P, spread=SPREAD):
+    """Surrogate inputs: log(p / template) / log(spread) of the active
+    parameters, in [-1, 1] for the search box."""
+    t = template()
+    idx = active_params()
+    return (np.log(P[:, idx] / t[idx]) / math.log(spread)).astype(np.float32)
+
+
+def synchrony(traj):
+    """Mean pairwise Pearson correlation across cells of traj [samples][cells]
+    (cells with a constant trace are left out), by
+    sum_{i != j} <z_i, z_j> = |sum_i z_i|^2 - sum_i |z_i|^2 on unit z_i."""
+    x = traj - traj.mean(axis=0, keepdims=True)
+    nrm = np.sqrt((x * x).sum(axis=0))
+    ok = nrm > 1e-12 * (1.0 + np.abs(traj).max())
+    n = int(ok.sum())
+    if n < 2:
+        return float("nan")
+    z = x[:, ok] / nrm[ok]
+    s = z.sum(axis=1)
+    return float(((s * s).sum() - n) / (n * (n - 1)))
+
+
+def simulate_features(P, minutes=120.0, cells=200, width=4, window=60.0, batch=4096, device=0,
+                      precision=E.FP64, log=None):
+    """Simulates every row of P (one set each) and returns its features."""
+    off, ids = default_graph(cells, width)
+    mh1 = workloads.her_species("mh1")
+    n = P.shape[0]
+    out = {k: np.full(n, np.nan) for k in ("period", "amplitude", "synchrony")}
+    out["status"] = np.zeros(n, np.int32)
+    t0 = time.perf_counter()
+    cell_steps = 0
+    for s in range(0, n, batch):
+        rows = P[s:s + batch]
+        sets = [E.ParameterSet(off, ids, p, duration=minutes) for p in rows]
+        an = [E.Analysis.oscillation(mh1, 0, cells, 0.0, window, 4.0, 0.1),
+              E.Analysis.trajectory(mh1, 0, cells, 0.0, window)]
+        b = E.Batch("her_model_2014", sets, 0.01, 0.1, an, precision=precision, device=device)
+        b.run()
+        b.sync()
+        st = b.status()
+        cell_steps += b.info()["total_cell_steps"]
+        for i in range(len(rows)):
+            o = b.oscillation(0, i)
+            with np.errstate(invalid="ignore"):
+                per = o["pers"][0]
+                amp = o["amps"][0]
+                out["period"][s + i] = np.nanmean(per) if np.isfinite(per).any() else np.nan
+                out["amplitude"][s + i] = np.nanmean(amp) if np.isfinite(amp).any() else np.nan
+            _, vals = b.trajectory(1, i)
+            out["synchrony"][s + i] = synchrony(vals[:, 0, :])
+            out["status"][s + i] = st[i]
+        b.close()
+        if log:
+            log("simulated %d / %d sets" % (min(s + batch, n), n))
+    out["oscillates"] = (np.isfinite(out["period"]) & (np.nan_to_num(out["amplitude"]) > OSC_AMP)).astype(np.float32)
+    out["seconds"] = time.perf_counter() - t0
+    out["cell_steps"] = cell_steps
+    return out
+
+
+def accepted(F):
+    per, amp = F["period"], F["amplitude"]
+    with np.errstate(invalid="ignore"):
+        return np.isfinite(per) & (np.abs(per - TARGET_PERIOD) <= PERIOD_TOL) & (np.nan_to_num(amp) >= AMP_MIN)
+
+
+def targets(F):
+    """Surrogate targets [n][5]: log period, log amplitude, synchrony, the
+    oscillation indicator and the acceptance indicator; and their mask
+    (feature defined)."""
+    with np.errstate(invalid="ignore", divide="ignore"):
+        T = np.stack([np.log(F["period"]), np.log(F["amplitude"]), F["synchrony"], F["oscillates"],
+                      accepted(F).astype(np.float64)], 1)
+    osc = F["oscillates"] > 0.5
+    one = np.ones_like(osc)
+    M = np.stack([osc, osc, np.isfinite(F["synchrony"]), one, one], 1).astype(np.float32)
+    M = M * np.isfinite(T)
+    return np.nan_to_num(T).astype(np.float32), M.astype(np.float32)
+
+
+def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None):
+    from .surrogate import MLP
+    X = encode(P)
+    T, M = targets(F)
+    net = MLP(X.shape[1], T.shape[1], seed=seed, lr=lr)
+    net.fit(X, T, M, epochs=epochs, batch=min(batch, (X.shape[0] // 128) * 128), seed=seed, log=log)
+    return net
+
+
+def predicted_score(pred):
+    """Higher is better: the predicted acceptance indicator, ties broken by
+    the predicted closeness to the period window."""
+    per = np.exp(np.clip(pred[:, 0], -10, 10))
+    return pred[:, 4] - 1e-3 * np.abs(per - TARGET_PERIOD) / PERIOD_TOL
+
+
+def feature_errors(net, P, F):
+    """Relative error of predicted period and amplitude on sets that
+    oscillate, against the FP64 simulation."""
+    pred = net.predict(encode(P))
+    osc = F["oscillates"] > 0.5
+    per_err = np.abs(np.exp(pred[osc, 0]) - F["period"][osc]) / F["period"][osc]
+    amp_err = np.abs(np.exp(pred[osc, 1]) - F["amplitude"][osc]) / F["amplitude"][osc]
+    return {"period_median": float(np.median(per_err)), "amplitude_median": float(np.median(amp_err)),
+            "period_p90": float(np.quantile(per_err, 0.9)), "amplitude_p90": float(np.quantile(amp_err, 0.9)),
+            "oscillation_accuracy": float(((pred[:, 3] > 0.5) == osc).mean()), "n": int(osc.sum())}
+
+
+def screened_search(net, n_candidates, seed, keep=0.01, plain_sample=4096, sim_kwargs=None, log=None):
+    """Surrogate-screened search against plain GPU search on the same
+    seeded candidates.  The surrogate ranks all candidates, its top `keep`
+    fraction is simulated in FP64 and accepted by the simulation alone; the
+    plain rate comes from simulating a random sample of the same candidates
+    and is extrapolated per candidate."""
+    sim_kwargs = sim_kwargs or {}
+    P = draw_candidates(n_candidates, seed)
+    t0 = time.perf_counter()
+    score = predicted_score(net.predict(encode(P)))
+    t_infer = time.perf_counter() - t0
+    top = np.argsort(-score, kind="stable")[:max(1, int(round(keep * n_candidates)))]
+    Fs = simulate_features(P[top], log=log, **sim_kwargs)
+    acc_s = accepted(Fs)
+    t_screen = t_infer + Fs["seconds"]
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    sample = rng.choice(n_candidates, size=min(plain_sample, n_candidates), replace=False)
+    Fp = simulate_features(P[sample], log=log, **sim_kwargs)
+    acc_p = accepted(Fp)
+    per_candidate = Fp["seconds"] / len(sample)
+    plain_rate = acc_p.mean() / per_candidate if acc_p.any() else 0.0
+    screened_rate = acc_s.sum() / t_screen
+    return {
+        "candidates": n_candidates, "kept": int(len(top)), "inference_s": t_infer,
+        "resimulation_s": Fs["seconds"], "accepted_screened": int(acc_s.sum()),
+        "false_accept_rate": float(1.0 - acc_s.mean()),
+        "plain_sample": int(len(sample)), "plain_accept_fraction": float(acc_p.mean()),
+        "plain_seconds_per_candidate": per_candidate,
+        "accepted_per_s_screened": float(screened_rate), "accepted_per_s_plain": float(plain_rate),
+        "gain": float(screened_rate / plain_rate) if plain_rate > 0 else float("inf"),
+    }
+
+
+class SRES:
+    """Stochastic-ranking evolution strategy (Runarsson & Yao, IEEE TEC 4(3),
+    2000), the method of DENSE's search/ (libSRES), in the log-parameter box
+    [-1, 1]^d of encode(): (mu, lambda) selection, self-adapted step sizes
+    with exponential smoothing (alpha), differential variation for the
+    parents (gamma).  The search is unconstrained, so stochastic ranking
+    reduces to sorting by fitness.
+
+    `fitness(X)` scores a whole population at once (one engine batch).
+    With a surrogate, `screen` x lambda offspring are drawn and only the
+    lambda the surrogate ranks best are scored by simulation.
+    """
+
+    def __init__(self, dim, fitness, mu=30, lam=200, seed=0, gamma=0.85, alpha=0.2, surrogate=None, screen=1):
+        self.dim, self.fitness, self.mu, self.lam = dim, fitness, mu, lam
+        self.gamma, self.alpha = gamma, alpha
+        self.rng = np.random.Generator(np.random.PCG64(seed))
+        self.tau = 1.0 / math.sqrt(2.0 * math.sqrt(dim))
+        self.tau_p = 1.0 / math.sqrt(2.0 * dim)
+        self.x = self.rng.uniform(-1, 1, size=(lam, dim))
+        self.sigma = np.full((lam, dim), 2.0 / math.sqrt(dim))
+        self.surrogate, self.screen = surrogate, max(1, screen)
+        self.f = self.fitness(self.x)
+        self.evaluations = lam
+
+    def step(self):
+        order = np.argsort(self.f, kind="stable")
+        par_x, par_s = self.x[order[:self.mu]], self.sigma[order[:self.mu]]
+        n_off = self.lam * self.screen
+        pick = np.arange(n_off) % self.mu
+        x, s = par_x[pick].copy(), par_s[pick].copy()
+        # differential variation of the mu - 1 best (the SRES recombination)
+        k = np.arange(n_off) < self.mu - 1
+        x[k] = x[k] + self.gamma * (par_x[0] - par_x[(np.arange(n_off)[k] + 1) % self.mu])
+        # self-adaptive mutation
+        n0 = self.rng.normal(size=(n_off, 1))
+        s_new = s * np.exp(self.tau_p * n0 + self.tau * self.rng.normal(size=s.shape))
+        s_new = np.clip(s_new, 1e-4, 2.0)
+        x_new = x + s_new * self.rng.normal(size=x.shape)
+        x_new = np.where(np.abs(x_new) > 1.0, x - 0.5 * (x_new - x), x_new)
+        x_new = np.clip(x_new, -1.0, 1.0)
+        s = s + self.alpha * (s_new - s)
+        if self.surrogate is not None and self.screen > 1:
+            keep = np.argsort(-self.surrogate(x_new), kind="stable")[:self.lam]
+            x_new, s = x_new[keep], s[keep]
+        self.x, self.sigma = x_new, s
+        self.f = self.fitness(self.x)
+        self.evaluations += len(self.x)
+        return float(np.min(self.f))
+
+
+def decode(X, spread=SPREAD):
+    """Inverse of encode: [n][d] in [-1, 1] -> full parameter rows."""
+    t = template()
+    P = np.tile(t, (X.shape[0], 1))
+    P[:, active_params()] = t[active_params()] * np.exp(X * math.log(spread))
+    return P
+
+
+def search_fitness(F):
+    """Lower is better: distance of the period to the target window, plus a
+    penalty below the amplitude threshold; sets that do not oscillate score 1e3."""
+    per, amp = F["period"], np.nan_to_num(F["amplitude"])
+    with np.errstate(invalid="ignore"):
+        f = np.abs(per - TARGET_PERIOD) / PERIOD_TOL + np.maximum(0.0, AMP_MIN - amp) / AMP_MIN
+    return np.where(np.isfinite(f), f, 1e3)

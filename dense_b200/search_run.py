@@ -1,0 +1,76 @@
+"""The surrogate experiment on one GPU, end to end:
+
+  1. draw seeded log-uniform +-4x candidates of her_model_2014 and simulate
+     a training set and a held-out set with the FP64 engine (features of
+     dense_b200.search);
+  2. train the MLP surrogate on the tensor-core kernels;
+  3. report the held-out feature error against the FP64 simulation;
+  4. surrogate-screened search on fresh candidates (top 1% re-simulated in
+     FP64) against plain GPU search on the same candidates (a random sample
+     simulated, rate extrapolated per candidate);
+  5. a few SRES generations with and without the surrogate in front of the
+     scorer.
+
+Prints one JSON object.  Usage:
+  python -m dense_b200.search_run [--train N] [--test N] [--candidates N]
+      [--minutes M] [--cells C] [--epochs E] [--generations G]
+"""
+
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import search as S
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=65536)
+    ap.add_argument("--test", type=int, default=4096)
+    ap.add_argument("--candidates", type=int, default=1000000)
+    ap.add_argument("--keep", type=float, default=0.01)
+    ap.add_argument("--plain-sample", type=int, default=4096)
+    ap.add_argument("--minutes", type=float, default=120.0)
+    ap.add_argument("--cells", type=int, default=200)
+    ap.add_argument("--epochs", type=int, default=120)
+    ap.add_argument("--generations", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=100)
+    a = ap.parse_args(argv)
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    sim = dict(minutes=a.minutes, cells=a.cells, width=4)
+    res = {"config": vars(a)}
+    t0 = time.perf_counter()
+    P_train = S.draw_candidates(a.train, a.seed)
+    F_train = S.simulate_features(P_train, log=log, **sim)
+    P_test = S.draw_candidates(a.test, a.seed + 1)
+    F_test = S.simulate_features(P_test, log=log, **sim)
+    res["data"] = {"train_sets": a.train, "test_sets": a.test, "seconds": F_train["seconds"] + F_test["seconds"],
+                   "cell_steps_per_s": (F_train["cell_steps"] + F_test["cell_steps"]) /
+                                       (F_train["seconds"] + F_test["seconds"]),
+                   "oscillating_fraction": float(F_train["oscillates"].mean()),
+                   "accepted_fraction": float(S.accepted(F_train).mean())}
+    t1 = time.perf_counter()
+    net = S.train_surrogate(P_train, F_train, epochs=a.epochs, batch=2048, seed=a.seed, log=log)
+    res["training_s"] = time.perf_counter() - t1
+    res["held_out_error"] = S.feature_errors(net, P_test, F_test)
+    res["search"] = S.screened_search(net, a.candidates, a.seed + 2, keep=a.keep, plain_sample=a.plain_sample,
+                                      sim_kwargs=sim, log=log)
+    if a.generations > 0:
+        fit = lambda X: S.search_fitness(S.simulate_features(S.decode(X), **sim))  # noqa: E731
+        pred = lambda X: S.predicted_score(net.predict(X.astype(np.float32)))  # noqa: E731
+        d = len(S.active_params())
+        for name, kw in (("plain", {}), ("screened", {"surrogate": pred, "screen": 8})):
+            es = S.SRES(d, fit, mu=16, lam=128, seed=a.seed, **kw)
+            best = [float(np.min(es.f))]
+            for _ in range(a.generations):
+                best.append(es.step())
+            res["sres_" + name] = {"best_fitness_per_generation": best, "simulations": es.evaluations}
+    res["total_s"] = time.perf_counter() - t0
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

