@@ -181,6 +181,11 @@ def screened_search(net, n_candidates, seed, keep=0.01, plain_sample=4096, sim_k
     top = np.argsort(-score, kind="stable")[:max(1, int(round(keep * n_candidates)))]
     Fs = simulate_features(P[top], log=log, **sim_kwargs)
     acc_s = accepted(Fs)
+    # surrogate error on the accepted sets, against their FP64 re-simulation
+    pred_top = net.predict(encode(P[top]))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        per_err = np.abs(np.exp(pred_top[acc_s, 0]) - Fs["period"][acc_s]) / Fs["period"][acc_s]
+        amp_err = np.abs(np.exp(pred_top[acc_s, 1]) - Fs["amplitude"][acc_s]) / Fs["amplitude"][acc_s]
     t_screen = t_infer + Fs["seconds"]
     rng = np.random.Generator(np.random.PCG64(seed + 1))
     sample = rng.choice(n_candidates, size=min(plain_sample, n_candidates), replace=False)
@@ -197,6 +202,8 @@ def screened_search(net, n_candidates, seed, keep=0.01, plain_sample=4096, sim_k
         "plain_seconds_per_candidate": per_candidate,
         "accepted_per_s_screened": float(screened_rate), "accepted_per_s_plain": float(plain_rate),
         "gain": float(screened_rate / plain_rate) if plain_rate > 0 else float("inf"),
+        "accepted_period_error_median": float(np.median(per_err)) if acc_s.any() else None,
+        "accepted_amplitude_error_median": float(np.median(amp_err)) if acc_s.any() else None,
     }
 
 

@@ -28,14 +28,14 @@ from . import search as S
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--train", type=int, default=65536)
+    ap.add_argument("--train", type=int, default=131072)
     ap.add_argument("--test", type=int, default=4096)
     ap.add_argument("--candidates", type=int, default=1000000)
     ap.add_argument("--keep", type=float, default=0.01)
     ap.add_argument("--plain-sample", type=int, default=4096)
     ap.add_argument("--minutes", type=float, default=120.0)
     ap.add_argument("--cells", type=int, default=200)
-    ap.add_argument("--epochs", type=int, default=120)
+    ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--generations", type=int, default=3)
     ap.add_argument("--seed", type=int, default=100)
     a = ap.parse_args(argv)

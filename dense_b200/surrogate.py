@@ -258,19 +258,28 @@ class MLP:
             self.k.adam(self.b[i], db[i], self.mb[i], self.vb[i], self.lr, self.steps)
         return loss
 
-    def fit(self, X, T, mask, epochs=20, batch=4096, seed=0, log=None):
+    def fit(self, X, T, mask, epochs=20, batch=4096, seed=0, log=None, cosine=True):
+        """Minibatch Adam; with `cosine` the learning rate follows a cosine
+        from lr down to lr/100 over the run."""
         rng = np.random.Generator(np.random.PCG64(seed))
         n = X.shape[0]
         hist = []
+        lr0 = self.lr
+        per_epoch = max(1, n // batch)
+        total = epochs * per_epoch
         for ep in range(epochs):
             order = rng.permutation(n)
             tot = 0.0
-            for s in range(0, n - batch + 1, batch):
+            for j, s in enumerate(range(0, n - batch + 1, batch)):
+                if cosine:
+                    t = (ep * per_epoch + j) / max(1, total - 1)
+                    self.lr = lr0 * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * t)))
                 idx = order[s:s + batch]
                 tot += self.step(X[idx], T[idx], mask[idx])
             hist.append(tot / max(1, n // batch))
             if log:
                 log("epoch %d loss %.5f" % (ep, hist[-1]))
+        self.lr = lr0
         return hist
 
     def state(self):
