@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -99,6 +100,7 @@ struct SetPlan {
   SetDesc d;
   int status = 0;
   bool use_mem = false;         // run by the memory-state kernel
+  int mem_block = 256;          // its CTA size
   std::vector<int> lvl_off;     // memory kernel: level offsets into lvl_cells
   std::vector<int> lvl_cells;   // memory kernel: cells in level order
 };
@@ -165,9 +167,19 @@ struct dense_engine {
   DeviceBuffer d_sets, d_prog, d_params, d_nbr_off, d_nbr_idx, d_state, d_ring, d_anl, d_init_conc,
       d_init_status, d_lists, d_lvl_off, d_lvl_cells;
   int n_reg = 0, n_mem = 0;  // sets run by the register / memory kernels (d_lists: reg then mem)
+  // memory-kernel sets grouped by CTA size: (threads, first index in the mem list, count)
+  std::vector<std::array<int, 3>> mem_groups;
   std::map<int, cudaGraphExec_t> graphs;
+  // the kernel launches of one run (register kernel, one per memory-kernel
+  // group) fork onto side streams so that they run concurrently
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev_join;
+  cudaEvent_t ev_fork = nullptr;
   ~dense_engine() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    for (auto& x : side) cudaStreamDestroy(x);
+    for (auto& x : ev_join) cudaEventDestroy(x);
+    if (ev_fork) cudaEventDestroy(ev_fork);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -181,7 +193,102 @@ int next_pow2(int x) {
   return p;
 }
 
+// Input checks of one set (CSR tissue, sizes, hints).
+int check_set(const dense_set_desc& in, const std::string& where) {
+  if (in.num_cells <= 0 || in.num_cells > kMaxCells)
+    return fail(DENSE_ERR_UNSUPPORTED, where + "1.." + std::to_string(kMaxCells) + " cells per set are supported");
+  if (!in.nbr_offsets || !in.nbr_ids || !in.set_params) return fail(DENSE_ERR_INVALID, where + "null input");
+  if (!(in.duration >= 0.0)) return fail(DENSE_ERR_INVALID, where + "negative duration");
+  const int n = in.num_cells;
+  if (in.nbr_offsets[0] != 0) return fail(DENSE_ERR_INVALID, where + "CSR offsets must start at 0");
+  for (int c = 0; c < n; ++c) {
+    if (in.nbr_offsets[c + 1] < in.nbr_offsets[c]) return fail(DENSE_ERR_INVALID, where + "CSR offsets decrease");
+    for (int k = in.nbr_offsets[c]; k < in.nbr_offsets[c + 1]; ++k) {
+      const int v = in.nbr_ids[k];
+      if (v < 0 || v >= n) return fail(DENSE_ERR_INVALID, where + "neighbour id outside the tissue");
+      if (k > in.nbr_offsets[c] && in.nbr_ids[k - 1] >= v)
+        return fail(DENSE_ERR_INVALID, where + "neighbour ids must ascend (DENSE keeps them in a std::set)");
+    }
+  }
+  if (in.schedule != DENSE_SCHEDULE_AUTO && in.schedule != DENSE_SCHEDULE_MEMORY)
+    return fail(DENSE_ERR_INVALID, where + "unknown schedule hint");
+  if (in.mem_block != 0 && (in.mem_block < 32 || in.mem_block > 256 || in.mem_block % 32))
+    return fail(DENSE_ERR_INVALID, where + "mem_block must be 32..256, a multiple of 32");
+  return DENSE_OK;
+}
+
+// The analyses of a run (analyses.xml entries) and the doubles of analysis
+// state each set of the batch holds.
+int build_analyses(const dense_run_desc* run, int num_sets, const dense_set_desc* in_sets,
+                   std::vector<AnalysisDesc>& out, int64_t& anl_block_out) {
+  const double interval = run->analysis_interval;
+  int min_cells = kMaxCells + 1;
+  for (int s = 0; s < num_sets; ++s) min_cells = std::min(min_cells, in_sets[s].num_cells);
+  int64_t anl_block = 0;
+  for (int ai = 0; ai < run->num_analyses; ++ai) {
+    const dense_analysis_desc& in = run->analyses[ai];
+    AnalysisDesc A{};
+    A.kind = in.kind;
+    A.cmin = in.cell_start;
+    A.cmax = in.cell_end;
+    A.t0 = in.time_start;
+    A.t1 = in.time_end;
+    if (A.cmin < 0 || A.cmax < A.cmin || A.cmax > min_cells)
+      return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": cell range outside the tissue");
+    if (in.kind == DENSE_ANALYSIS_CONCCHECK && in.num_species == 0) {
+      A.nsp = NUM_SPECIES;
+      for (int i = 0; i < NUM_SPECIES; ++i) A.sp[i] = i;
+    } else {
+      if (in.num_species <= 0 || in.num_species > NUM_SPECIES || !in.species)
+        return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": bad species list");
+      A.nsp = in.num_species;
+      for (int i = 0; i < in.num_species; ++i) {
+        if (in.species[i] < 0 || in.species[i] >= NUM_SPECIES)
+          return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": bad species id");
+        A.sp[i] = in.species[i];
+      }
+    }
+    const int64_t m = A.cmax - A.cmin;
+    A.off = anl_block;
+    if (in.kind == DENSE_ANALYSIS_BASIC) {
+      anl_block += 3 * A.nsp + 2 + 3 * m * A.nsp;
+    } else if (in.kind == DENSE_ANALYSIS_OSCILLATION) {
+      if (!(in.anlys_intvl > 0.0) || !(in.win_range >= 0.0))
+        return fail(DENSE_ERR_INVALID, "oscillation: bad window");
+      const double rs = in.win_range / in.anlys_intvl;  // oscillation.hpp:64
+      if (!(rs < 1e6)) return fail(DENSE_ERR_UNSUPPORTED, "oscillation window too long");
+      A.range_steps = static_cast<int>(rs);
+      A.interval = in.anlys_intvl;
+      anl_block += 2 + m * A.nsp * kOscFields + static_cast<int64_t>(A.nsp) * (A.range_steps + 1) * m;
+    } else if (in.kind == DENSE_ANALYSIS_CONCCHECK) {
+      A.lo = in.lower;
+      A.hi = in.upper;
+      anl_block += 1;
+    } else if (in.kind == DENSE_ANALYSIS_TRAJECTORY) {
+      // room for every sample inside [time_start, time_end) of the longest
+      // horizon in the batch
+      int cap = 0;
+      for (int s = 0; s < num_sets; ++s) {
+        const double t1 = std::min(in.time_end, in_sets[s].duration), t0 = std::max(in.time_start, 0.0);
+        const int all = static_cast<int>(std::ceil(in_sets[s].duration / interval));
+        const int in_window = t1 > t0 ? static_cast<int>(std::ceil((t1 - t0) / interval)) + 2 : 0;
+        cap = std::max(cap, std::min(all, in_window));
+      }
+      A.range_steps = cap;
+      anl_block += 2 + cap + static_cast<int64_t>(cap) * A.nsp * m;
+    } else {
+      return fail(DENSE_ERR_INVALID, "unknown analysis kind");
+    }
+    anl_block = (anl_block + 1) & ~int64_t(1);
+    out.push_back(A);
+  }
+
+  anl_block_out = anl_block;
+  return DENSE_OK;
+}
+
 int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<double>& cell_params) {
+  const bool force_mem = in.schedule == DENSE_SCHEDULE_MEMORY;
   const int n = in.num_cells;
   SetDesc& d = plan.d;
   d.n_cells = n;
@@ -244,8 +351,12 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
   // sets larger than a CTA, run in the memory-state kernel, which keeps
   // every species in its ring (at least two rows)
   d.ordered = ordered ? 1 : 0;
-  plan.use_mem = ordered || n > kStepThreads;
+  plan.use_mem = ordered || n > kStepThreads || force_mem;
   plan_levels(in, ordered, plan);
+  // memory-kernel CTA size: the hint, else the widest level in warps (32..256)
+  int widest = 0;
+  for (size_t l = 0; l + 1 < plan.lvl_off.size(); ++l) widest = std::max(widest, plan.lvl_off[l + 1] - plan.lvl_off[l]);
+  plan.mem_block = in.mem_block > 0 ? in.mem_block : std::min(256, std::max(32, (widest + 31) / 32 * 32));
   int64_t off = 0;
   for (int sp = 0; sp < NUM_SPECIES; ++sp) {
     int depth = 0;
@@ -308,65 +419,10 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   CUDA_TRY(cudaSetDevice(run->device));
 
   // ---- analyses
-  int min_cells = kMaxCells + 1;
-  for (int s = 0; s < num_sets; ++s) min_cells = std::min(min_cells, in_sets[s].num_cells);
   int64_t anl_block = 0;
-  for (int ai = 0; ai < run->num_analyses; ++ai) {
-    const dense_analysis_desc& in = run->analyses[ai];
-    AnalysisDesc A{};
-    A.kind = in.kind;
-    A.cmin = in.cell_start;
-    A.cmax = in.cell_end;
-    A.t0 = in.time_start;
-    A.t1 = in.time_end;
-    if (A.cmin < 0 || A.cmax < A.cmin || A.cmax > min_cells)
-      return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": cell range outside the tissue");
-    if (in.kind == DENSE_ANALYSIS_CONCCHECK && in.num_species == 0) {
-      A.nsp = NUM_SPECIES;
-      for (int i = 0; i < NUM_SPECIES; ++i) A.sp[i] = i;
-    } else {
-      if (in.num_species <= 0 || in.num_species > NUM_SPECIES || !in.species)
-        return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": bad species list");
-      A.nsp = in.num_species;
-      for (int i = 0; i < in.num_species; ++i) {
-        if (in.species[i] < 0 || in.species[i] >= NUM_SPECIES)
-          return fail(DENSE_ERR_INVALID, "analysis " + std::to_string(ai) + ": bad species id");
-        A.sp[i] = in.species[i];
-      }
-    }
-    const int64_t m = A.cmax - A.cmin;
-    A.off = anl_block;
-    if (in.kind == DENSE_ANALYSIS_BASIC) {
-      anl_block += 3 * A.nsp + 2 + 3 * m * A.nsp;
-    } else if (in.kind == DENSE_ANALYSIS_OSCILLATION) {
-      if (!(in.anlys_intvl > 0.0) || !(in.win_range >= 0.0))
-        return fail(DENSE_ERR_INVALID, "oscillation: bad window");
-      const double rs = in.win_range / in.anlys_intvl;  // oscillation.hpp:64
-      if (!(rs < 1e6)) return fail(DENSE_ERR_UNSUPPORTED, "oscillation window too long");
-      A.range_steps = static_cast<int>(rs);
-      A.interval = in.anlys_intvl;
-      anl_block += 2 + m * A.nsp * kOscFields + static_cast<int64_t>(A.nsp) * (A.range_steps + 1) * m;
-    } else if (in.kind == DENSE_ANALYSIS_CONCCHECK) {
-      A.lo = in.lower;
-      A.hi = in.upper;
-      anl_block += 1;
-    } else if (in.kind == DENSE_ANALYSIS_TRAJECTORY) {
-      // room for every sample inside [time_start, time_end) of the longest
-      // horizon in the batch
-      int cap = 0;
-      for (int s = 0; s < num_sets; ++s) {
-        const double t1 = std::min(in.time_end, in_sets[s].duration), t0 = std::max(in.time_start, 0.0);
-        const int all = static_cast<int>(std::ceil(in_sets[s].duration / interval));
-        const int in_window = t1 > t0 ? static_cast<int>(std::ceil((t1 - t0) / interval)) + 2 : 0;
-        cap = std::max(cap, std::min(all, in_window));
-      }
-      A.range_steps = cap;
-      anl_block += 2 + cap + static_cast<int64_t>(cap) * A.nsp * m;
-    } else {
-      return fail(DENSE_ERR_INVALID, "unknown analysis kind");
-    }
-    anl_block = (anl_block + 1) & ~int64_t(1);
-    e->analyses.push_back(A);
+  {
+    const int rc = build_analyses(run, num_sets, in_sets, e->analyses, anl_block);
+    if (rc != DENSE_OK) return rc;
   }
 
   // ---- sets
@@ -374,28 +430,18 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   std::vector<int> off_all, idx_all;
   int64_t cells_total = 0, ring_total = 0;
   int max_cells = 0, max_edges = 0;
-  std::vector<int> reg_list, mem_list, lvl_off_all, lvl_cells_all;
+  std::vector<int> reg_list, mem_list, mem_block_of, lvl_off_all, lvl_cells_all;
   e->sets.resize(num_sets);
   e->init_status.resize(num_sets);
   std::vector<double> cp;
   for (int s = 0; s < num_sets; ++s) {
     const dense_set_desc& in = in_sets[s];
     const std::string where = "set " + std::to_string(s) + ": ";
-    if (in.num_cells <= 0 || in.num_cells > kMaxCells)
-      return fail(DENSE_ERR_UNSUPPORTED, where + "1.." + std::to_string(kMaxCells) + " cells per set are supported");
-    if (!in.nbr_offsets || !in.nbr_ids || !in.set_params) return fail(DENSE_ERR_INVALID, where + "null input");
-    if (!(in.duration >= 0.0)) return fail(DENSE_ERR_INVALID, where + "negative duration");
-    const int n = in.num_cells;
-    if (in.nbr_offsets[0] != 0) return fail(DENSE_ERR_INVALID, where + "CSR offsets must start at 0");
-    for (int c = 0; c < n; ++c) {
-      if (in.nbr_offsets[c + 1] < in.nbr_offsets[c]) return fail(DENSE_ERR_INVALID, where + "CSR offsets decrease");
-      for (int k = in.nbr_offsets[c]; k < in.nbr_offsets[c + 1]; ++k) {
-        const int v = in.nbr_ids[k];
-        if (v < 0 || v >= n) return fail(DENSE_ERR_INVALID, where + "neighbour id outside the tissue");
-        if (k > in.nbr_offsets[c] && in.nbr_ids[k - 1] >= v)
-          return fail(DENSE_ERR_INVALID, where + "neighbour ids must ascend (DENSE keeps them in a std::set)");
-      }
+    {
+      const int rc = check_set(in, where);
+      if (rc != DENSE_OK) return rc;
     }
+    const int n = in.num_cells;
     SetPlan plan;
     int rc = plan_set(in, dt, plan, cp);
     if (rc != DENSE_OK) return fail(rc, where + g_error);
@@ -424,6 +470,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     ring_total = (ring_total + 31) & ~int64_t(31);
     if (plan.use_mem) {
       mem_list.push_back(s);
+      mem_block_of.push_back(plan.mem_block);
       d.lvl_base = static_cast<int64_t>(lvl_off_all.size());
       lvl_off_all.insert(lvl_off_all.end(), plan.lvl_off.begin(), plan.lvl_off.end());
     } else {
@@ -463,7 +510,18 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     };
     auto by_cost = [&](int x, int y) { return cost(x) != cost(y) ? cost(x) > cost(y) : x < y; };
     std::stable_sort(reg_list.begin(), reg_list.end(), by_cost);
-    std::stable_sort(mem_list.begin(), mem_list.end(), by_cost);
+    // memory-kernel sets: grouped by CTA size, longest first in a group
+    std::vector<int> blk_of(num_sets, 0);
+    for (size_t k = 0; k < mem_list.size(); ++k) blk_of[mem_list[k]] = mem_block_of[k];
+    std::stable_sort(mem_list.begin(), mem_list.end(), [&](int x, int y) {
+      return blk_of[x] != blk_of[y] ? blk_of[x] < blk_of[y] : by_cost(x, y);
+    });
+    for (size_t k = 0; k < mem_list.size(); ++k) {
+      const int b = blk_of[mem_list[k]];
+      if (e->mem_groups.empty() || e->mem_groups.back()[0] != b)
+        e->mem_groups.push_back({b, static_cast<int>(k), 0});
+      e->mem_groups.back()[2]++;
+    }
     std::vector<int> lists(reg_list);
     lists.insert(lists.end(), mem_list.begin(), mem_list.end());
     CUDA_TRY(cudaMemcpyAsync(e->d_lists.p, lists.data(), sizeof(int) * num_sets, cudaMemcpyHostToDevice, e->stream));
@@ -473,6 +531,18 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     CUDA_TRY(cudaMemcpyAsync(e->d_lvl_cells.p, lvl_cells_all.data(), sizeof(int) * lvl_cells_all.size(),
                              cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
+  }
+  const int n_launch = (e->n_reg > 0 ? 1 : 0) + static_cast<int>(e->mem_groups.size());
+  if (n_launch > 1) {
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    for (int i = 1; i < n_launch; ++i) {
+      cudaStream_t x;
+      cudaEvent_t ev;
+      CUDA_TRY(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      e->side.push_back(x);
+      CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      e->ev_join.push_back(ev);
+    }
   }
   CUDA_TRY(cudaMemcpyAsync(e->d_sets.p, e->sets.data(), sizeof(SetDesc) * num_sets, cudaMemcpyHostToDevice, e->stream));
   std::vector<float> params_f;
@@ -550,14 +620,47 @@ int dense_engine_reset(dense_engine* e, void* stream) {
   return DENSE_OK;
 }
 
+// One run: the register kernel over its sets, and the memory kernel once
+// per CTA-size group.  With more than one launch, every launch after the
+// first goes to a side stream forked from `s` and joined back into it, so
+// the kernels share the GPU instead of running one after the other (in a
+// captured graph they become parallel branches).
 static cudaError_t launch_all(dense_engine* e, const StepArgs& a, cudaStream_t s) {
   const int* reg = static_cast<const int*>(e->d_lists.p);
   const int* mem = reg + e->n_reg;
-  cudaError_t r = e->precision == DENSE_FP64 ? launch_step_fp64(a, reg, e->n_reg, e->smem, s)
-                                              : launch_step_fp32(a, reg, e->n_reg, e->smem, s);
-  if (r != cudaSuccess) return r;
-  return e->precision == DENSE_FP64 ? launch_step_mem_fp64(a, mem, e->n_mem, s)
-                                    : launch_step_mem_fp32(a, mem, e->n_mem, s);
+  const bool fork = !e->side.empty();
+  cudaError_t r;
+  if (fork && (r = cudaEventRecord(e->ev_fork, s)) != cudaSuccess) return r;
+  int k = 0;  // launches issued so far
+  auto stream_for = [&](cudaStream_t& st) -> cudaError_t {
+    st = (fork && k > 0) ? e->side[k - 1] : s;
+    return st != s ? cudaStreamWaitEvent(st, e->ev_fork, 0) : cudaSuccess;
+  };
+  auto join = [&](cudaStream_t st) -> cudaError_t {
+    cudaError_t rj = cudaSuccess;
+    if (st != s) {
+      rj = cudaEventRecord(e->ev_join[k - 1], st);
+      if (rj == cudaSuccess) rj = cudaStreamWaitEvent(s, e->ev_join[k - 1], 0);
+    }
+    ++k;
+    return rj;
+  };
+  cudaStream_t st;
+  if (e->n_reg > 0) {
+    if ((r = stream_for(st)) != cudaSuccess) return r;
+    r = e->precision == DENSE_FP64 ? launch_step_fp64(a, reg, e->n_reg, e->smem, st)
+                                   : launch_step_fp32(a, reg, e->n_reg, e->smem, st);
+    if (r != cudaSuccess) return r;
+    if ((r = join(st)) != cudaSuccess) return r;
+  }
+  for (const auto& g : e->mem_groups) {
+    if ((r = stream_for(st)) != cudaSuccess) return r;
+    r = e->precision == DENSE_FP64 ? launch_step_mem_fp64(a, mem + g[1], g[2], g[0], st)
+                                   : launch_step_mem_fp32(a, mem + g[1], g[2], g[0], st);
+    if (r != cudaSuccess) return r;
+    if ((r = join(st)) != cudaSuccess) return r;
+  }
+  return cudaSuccess;
 }
 
 int dense_engine_run(dense_engine* e, int num_chunks, void* stream) {
@@ -756,6 +859,40 @@ int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D) {
   for (int sp = 0; sp < NUM_SPECIES; ++sp) {
     if (S) S[sp] = e->sets[set].S[sp];
     if (D) D[sp] = e->sets[set].D[sp];
+  }
+  return DENSE_OK;
+}
+
+// Per-set device bytes and kernel of a batch, from the same planning as
+// dense_engine_create, without touching the GPU.
+int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_desc* in_sets, int64_t* set_bytes,
+                      int* set_kernel) {
+  if (!run || num_sets <= 0 || !in_sets) return fail(DENSE_ERR_INVALID, "null argument or no sets");
+  if (!(run->step_size > 0.0) || !(run->analysis_interval > 0.0))
+    return fail(DENSE_ERR_INVALID, "step size and analysis interval must be positive");
+  if (run->precision != DENSE_FP64 && run->precision != DENSE_FP32_KAHAN)
+    return fail(DENSE_ERR_INVALID, "unknown precision");
+  if (run->num_analyses < 0 || run->num_analyses > kMaxAnalyses)
+    return fail(DENSE_ERR_UNSUPPORTED, "at most " + std::to_string(kMaxAnalyses) + " analyses per batch");
+  std::vector<AnalysisDesc> analyses;
+  int64_t anl_block = 0;
+  int rc = build_analyses(run, num_sets, in_sets, analyses, anl_block);
+  if (rc != DENSE_OK) return rc;
+  const int64_t tsz = run->precision == DENSE_FP64 ? 8 : 4;
+  std::vector<double> cp;
+  for (int s = 0; s < num_sets; ++s) {
+    const dense_set_desc& in = in_sets[s];
+    const std::string where = "set " + std::to_string(s) + ": ";
+    if ((rc = check_set(in, where)) != DENSE_OK) return rc;
+    SetPlan plan;
+    if ((rc = plan_set(in, run->step_size, plan, cp)) != DENSE_OK) return fail(rc, where + g_error);
+    const int64_t n = in.num_cells;
+    if (set_bytes)
+      set_bytes[s] = tsz * (((ring_elems(plan.d) + 31) & ~int64_t(31)) + 2 * NUM_SPECIES * n +
+                            static_cast<int64_t>(cp.size())) +
+                     4 * (n + 1 + in.nbr_offsets[n] + static_cast<int64_t>(plan.lvl_off.size()) + n + 2) +
+                     8 * (anl_block + NUM_SPECIES) + static_cast<int64_t>(sizeof(SetDesc) + sizeof(SetProgress));
+    if (set_kernel) set_kernel[s] = plan.use_mem ? plan.mem_block : 0;
   }
   return DENSE_OK;
 }

@@ -743,10 +743,10 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
 
   const int pstride = sd.param_stride;
   const T* P = static_cast<const T*>(a.params) + sd.param_base;
-  if (tid < kNS) {
-    s_S[tid] = sd.S[tid];
-    s_mask[tid] = sd.D[tid] - 1;
-    s_roff[tid] = sd.ring_off[tid];
+  for (int i = tid; i < kNS; i += blk) {  // blocks may be a single warp
+    s_S[i] = sd.S[i];
+    s_mask[i] = sd.D[i] - 1;
+    s_roff[i] = sd.ring_off[i];
   }
   if (pstride == 0)
     for (int i = tid; i < kNP; i += blk) s_prm[i] = P[i];
@@ -776,9 +776,9 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
 
   for (; chunk < chunk_end; ++chunk) {
     if (a.n_analyses > 0) {
-      if (tid < kNS) {
-        const int row = a.val_slot[tid];
-        if (row >= 0) s_rows[row] = ring + s_roff[tid] + static_cast<int64_t>(step & s_mask[tid]) * n;
+      for (int i = tid; i < kNS; i += blk) {
+        const int row = a.val_slot[i];
+        if (row >= 0) s_rows[row] = ring + s_roff[i] + static_cast<int64_t>(step & s_mask[i]) * n;
       }
       __syncthreads();
       const bool bad = analyses_sample(a, anl, RingVals<T>{s_rows}, tid, tid, blk, n, age, s_samples);
@@ -953,12 +953,12 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
     return cudaGetLastError();                                                                  \
   }                                                                                             \
   cudaError_t launch_step_mem_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets,       \
-                                       cudaStream_t s) {                                        \
+                                       int block, cudaStream_t s) {                             \
     if (n_sets <= 0) return cudaSuccess;                                                        \
     if (a.uniform_params)                                                                       \
-      dense_step_mem_kernel<T, KAHAN, true><<<n_sets, 256, 0, s>>>(a, set_list);                 \
+      dense_step_mem_kernel<T, KAHAN, true><<<n_sets, block, 0, s>>>(a, set_list);               \
     else                                                                                        \
-      dense_step_mem_kernel<T, KAHAN, false><<<n_sets, 256, 0, s>>>(a, set_list);                \
+      dense_step_mem_kernel<T, KAHAN, false><<<n_sets, block, 0, s>>>(a, set_list);              \
     return cudaGetLastError();                                                                  \
   }                                                                                             \
   cudaError_t launch_step_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets, size_t smem, \

@@ -28,6 +28,8 @@ SET_NAN_PARAM = 2
 SET_UNSTAGED_LAG = 4
 SET_BAD_DELAY = 8
 SET_ORDERED_READS = 16
+SCHEDULE_AUTO = 0
+SCHEDULE_MEMORY = 1
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
@@ -40,7 +42,8 @@ class _ModelInfo(C.Structure):
 
 class _SetDesc(C.Structure):
     _fields_ = [("num_cells", C.c_int), ("nbr_offsets", _I), ("nbr_ids", _I), ("set_params", _D),
-                ("cell_params", _D), ("init_conc", _D), ("perturb", _D), ("duration", C.c_double)]
+                ("cell_params", _D), ("init_conc", _D), ("perturb", _D), ("duration", C.c_double),
+                ("schedule", C.c_int), ("mem_block", C.c_int)]
 
 
 class _AnalysisDesc(C.Structure):
@@ -61,6 +64,7 @@ _FUNCS = {
     "dense_model_reaction_name": (C.c_char_p, [C.c_int]),
     "dense_last_error": (C.c_char_p, []),
     "dense_engine_create": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_void_p)]),
+    "dense_engine_plan": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_int64), _I]),
     "dense_engine_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dense_engine_run_graph": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dense_engine_sync": (C.c_int, [C.c_void_p]),
@@ -129,7 +133,7 @@ class ParameterSet:
     """One DENSE simulation: tissue, parameters, initial state, horizon."""
 
     def __init__(self, nbr_offsets, nbr_ids, set_params, cell_params=None, init_conc=None, perturb=None,
-                 duration=0.0):
+                 duration=0.0, schedule=0, mem_block=0):
         self.nbr_offsets = np.ascontiguousarray(nbr_offsets, np.int32)
         self.nbr_ids = np.ascontiguousarray(nbr_ids, np.int32)
         self.num_cells = len(self.nbr_offsets) - 1
@@ -138,6 +142,9 @@ class ParameterSet:
         self.init_conc = None if init_conc is None else np.ascontiguousarray(init_conc, np.float64)
         self.perturb = None if perturb is None else np.ascontiguousarray(perturb, np.float64)
         self.duration = float(duration)
+        # schedule hints (SCHEDULE_*, memory-kernel CTA size); results do not depend on them
+        self.schedule = int(schedule)
+        self.mem_block = int(mem_block)
 
 
 class Analysis:
@@ -178,6 +185,54 @@ def _ip(a):
     return None if a is None else a.ctypes.data_as(_I)
 
 
+def _describe(L, sets, analyses, step_size, analysis_interval, precision, device):
+    """C descriptors of a batch: (run desc, set desc array, arrays to keep alive)."""
+    keep = []
+    cset = (_SetDesc * len(sets))()
+    for i, s in enumerate(sets):
+        if s.cell_params is not None and s.cell_params.size != s.num_cells * L.num_params:
+            raise DenseError("cell_params must be [num_cells][num_params]")
+        if s.set_params.size != L.num_params:
+            raise DenseError("set_params must have %d values" % L.num_params)
+        cset[i].num_cells = s.num_cells
+        cset[i].nbr_offsets = _ip(s.nbr_offsets)
+        cset[i].nbr_ids = _ip(s.nbr_ids)
+        cset[i].set_params = _dp(s.set_params)
+        cset[i].cell_params = _dp(s.cell_params)
+        cset[i].init_conc = _dp(s.init_conc)
+        cset[i].perturb = _dp(s.perturb)
+        cset[i].duration = s.duration
+        cset[i].schedule = s.schedule
+        cset[i].mem_block = s.mem_block
+    can = (_AnalysisDesc * max(1, len(analyses)))()
+    for i, a in enumerate(analyses):
+        sp = np.ascontiguousarray(L.species_ids(a.species), np.int32)
+        keep.append(sp)
+        can[i].kind = a.kind
+        can[i].num_species = len(sp)
+        can[i].species = _ip(sp) if len(sp) else None
+        can[i].cell_start, can[i].cell_end = a.cell_start, a.cell_end
+        can[i].time_start, can[i].time_end = a.time_start, a.time_end
+        can[i].win_range, can[i].anlys_intvl = a.win_range, a.anlys_intvl
+        can[i].lower, can[i].upper = a.lower, a.upper
+    run = _RunDesc(precision, float(step_size), float(analysis_interval), len(analyses), can, device)
+    return run, cset, keep
+
+
+def plan(model, sets, step_size, analysis_interval, analyses=(), precision=FP64):
+    """Per-set device bytes and kernel (0 = register kernel, else the
+    memory-state kernel's CTA size) that a Batch of these sets would use;
+    needs no GPU."""
+    L = load(model) if isinstance(model, str) else model
+    sets = list(sets)
+    run, cset, keep = _describe(L, sets, list(analyses), step_size, analysis_interval, precision, 0)
+    nbytes = np.zeros(len(sets), np.int64)
+    kernel = np.zeros(len(sets), np.int32)
+    L._check(L.lib.dense_engine_plan(C.byref(run), len(sets), cset, nbytes.ctypes.data_as(C.POINTER(C.c_int64)),
+                                     _ip(kernel)))
+    return nbytes, kernel
+
+
 class Batch:
     """A batch of parameter sets staged on one GPU (dense_engine)."""
 
@@ -187,33 +242,8 @@ class Batch:
         self.analyses = list(analyses)
         self.precision = precision
         L = self.L
-        self._keep = []
-        cset = (_SetDesc * len(self.sets))()
-        for i, s in enumerate(self.sets):
-            if s.cell_params is not None and s.cell_params.size != s.num_cells * L.num_params:
-                raise DenseError("cell_params must be [num_cells][num_params]")
-            if s.set_params.size != L.num_params:
-                raise DenseError("set_params must have %d values" % L.num_params)
-            cset[i].num_cells = s.num_cells
-            cset[i].nbr_offsets = _ip(s.nbr_offsets)
-            cset[i].nbr_ids = _ip(s.nbr_ids)
-            cset[i].set_params = _dp(s.set_params)
-            cset[i].cell_params = _dp(s.cell_params)
-            cset[i].init_conc = _dp(s.init_conc)
-            cset[i].perturb = _dp(s.perturb)
-            cset[i].duration = s.duration
-        can = (_AnalysisDesc * max(1, len(self.analyses)))()
-        for i, a in enumerate(self.analyses):
-            sp = np.ascontiguousarray(L.species_ids(a.species), np.int32)
-            self._keep.append(sp)
-            can[i].kind = a.kind
-            can[i].num_species = len(sp)
-            can[i].species = _ip(sp) if len(sp) else None
-            can[i].cell_start, can[i].cell_end = a.cell_start, a.cell_end
-            can[i].time_start, can[i].time_end = a.time_start, a.time_end
-            can[i].win_range, can[i].anlys_intvl = a.win_range, a.anlys_intvl
-            can[i].lower, can[i].upper = a.lower, a.upper
-        run = _RunDesc(precision, float(step_size), float(analysis_interval), len(self.analyses), can, device)
+        run, cset, self._keep = _describe(L, self.sets, self.analyses, step_size, analysis_interval, precision,
+                                          device)
         h = C.c_void_p()
         L._check(L.lib.dense_engine_create(C.byref(run), len(self.sets), cset, C.byref(h)))
         self.h = h

@@ -62,6 +62,10 @@ extern "C" {
 #define DENSE_SET_BAD_DELAY 8      /* a delay DENSE would read out of bounds with */
 #define DENSE_SET_ORDERED_READS 16 /* neighbour reads of rows written in the same step */
 
+/* schedule hint of a set (dense_set_desc.schedule) */
+#define DENSE_SCHEDULE_AUTO 0    /* register kernel when the set fits one, else memory kernel */
+#define DENSE_SCHEDULE_MEMORY 1  /* memory-state kernel */
+
 /* arithmetic of a batch */
 #define DENSE_FP64 0        /* matches DENSE's CPU path bit for bit */
 #define DENSE_FP32_KAHAN 1  /* FP32 rates, Kahan-compensated FP32 state */
@@ -82,7 +86,7 @@ typedef struct dense_model_info {
 
 /* One parameter set (one DENSE Simulation). */
 typedef struct dense_set_desc {
-  int num_cells;              /* <= 1024 */
+  int num_cells;              /* <= 65536 */
   const int* nbr_offsets;     /* [num_cells + 1] CSR row offsets */
   const int* nbr_ids;         /* neighbour cell ids, ascending per cell (std::set order) */
   const double* set_params;   /* [num_params]: the Parameter_Set; ring sizes derive from it */
@@ -91,6 +95,10 @@ typedef struct dense_set_desc {
   const double* init_conc;    /* [num_species] initial value of every history row, or NULL (zeros) */
   const double* perturb;      /* [num_reactions] -b factors entering the ring sizes, or NULL */
   double duration;            /* simulated minutes (-t) */
+  /* Schedule hints, 0 = the engine's choice (results do not depend on them;
+     dense_b200.autotune picks them by timing): */
+  int schedule;               /* DENSE_SCHEDULE_MEMORY: run the set in the memory-state kernel */
+  int mem_block;              /* memory-state kernel threads per CTA: 32..256, a multiple of 32 */
 } dense_set_desc;
 
 /* One analysis, applied to every set (an <anlys> entry of analyses.xml). */
@@ -178,6 +186,15 @@ DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int6
 DENSE_API int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D);
 
 DENSE_API int dense_engine_destroy(dense_engine* e);
+
+/* Planning without a GPU (no counterpart in DENSE, whose Simulation objects
+   size themselves, sim/base.cpp:55-140): per set, the device bytes
+   dense_engine_create would hold for it (set_bytes, or NULL) and the kernel
+   it would run in (set_kernel: 0 = register kernel, else the memory-state
+   kernel's threads per CTA; or NULL).  Used to cut batches into waves that
+   fit the device. */
+DENSE_API int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_desc* sets,
+                                int64_t* set_bytes, int* set_kernel);
 
 /* No counterpart in DENSE: an addition of this library for callers that may
    not allocate device memory -- code running inside a framework that owns

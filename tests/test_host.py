@@ -75,3 +75,34 @@ def test_report_number_format():
     assert report.fmt(float("nan")) == "nan"
     assert report.fmt(-float("nan")) == "-nan"
     assert report.fmt(1e-7) == "1e-07"
+
+
+def test_plan_kernels_and_bytes():
+    """dense_engine_plan (no GPU): register kernel for unordered sets of at
+    most 256 cells, memory kernel above that or on request, a CTA the width
+    of the widest dependency level for ordered (Turing) sets, hints checked."""
+    from dense_b200 import tissue, workloads
+    from dense_b200.engine import DenseError, ParameterSet, SCHEDULE_MEMORY, plan
+    p = workloads.template_params()
+    sets = []
+    for n in (16, 256, 300, 1024):
+        off, ids = tissue.default_graph(n, 4)
+        sets.append(ParameterSet(off, ids, p, duration=100))
+    off, ids = tissue.default_graph(200, 4)
+    sets.append(ParameterSet(off, ids, p, duration=100, schedule=SCHEDULE_MEMORY))
+    sets.append(ParameterSet(off, ids, p, duration=100, schedule=SCHEDULE_MEMORY, mem_block=96))
+    nbytes, kernel = plan("her_model_2014", sets, 0.01, 1.0)
+    assert list(kernel) == [0, 0, 256, 256, 224, 96]
+    assert (np.diff(nbytes[:4]) > 0).all() and nbytes[4] == nbytes[5]
+    tp = workloads.template_params("turing")
+    ts = []
+    for N in (8, 16, 64):
+        off, ids = tissue.default_graph(N * N, N)
+        ts.append(ParameterSet(off, ids, tp, duration=10))
+    _, kernel = plan("turing", ts, 0.01, 1.0)
+    assert list(kernel) == [32, 32, 32]
+    with pytest.raises(DenseError):
+        plan("her_model_2014", [ParameterSet(off, ids, tp, duration=10)], 0.01, 1.0)
+    off, ids = tissue.default_graph(200, 4)
+    with pytest.raises(DenseError):
+        plan("her_model_2014", [ParameterSet(off, ids, p, duration=10, mem_block=48)], 0.01, 1.0)
