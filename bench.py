@@ -136,6 +136,157 @@ def cpu_sample(kind_pref="reference", num_sets=2, minutes=300.0, seed=7):
                       "one host core, %.1f s" % (num_sets, minutes, dt)}
 
 
+# Turing-Pattern cell-step: 4 species read and written (8 B each); the
+# neighbour averages read rows of the same arrays, so they add no distinct
+# bytes.
+TURING_BYTES_PER_CELL_STEP = 64
+MIXED_BYTES = {"her_model_2014": BYTES_PER_CELL_STEP, "turing": TURING_BYTES_PER_CELL_STEP}
+MIXED_WORKLOAD = ("uneven mixed batch, one captured graph: %d sets, her_model_2014 (cells log-uniform 16..1024, "
+                  "-w 4, delays U[5,20] min) or Turing-Pattern (N x N grid, N U[8,64], -w N) with probability 1/2, "
+                  "horizons U[100,1200] min, every rate x exp(U(ln .5, ln 2)), dt 0.01 min, no analyses, "
+                  "autotuned schedules")
+
+
+def mixed_cpu_sample(groups, minutes=20.0, per_model=2):
+    """DENSE's own CPU path (oracle/_ref) on `per_model` sets of each model
+    of the mixed batch, `minutes` each, one host core."""
+    from oracle.pyoracle import load_oracle, load_ref
+    kinds, steps = set(), 0
+    t0 = time.perf_counter()
+    for m, sets in groups.items():
+        lib = load_ref(m)
+        kind = "reference"
+        if lib is None:
+            lib, kind = load_oracle(m), "port"
+        kinds.add(kind)
+        for ps in sets[:per_model]:
+            cp = np.tile(ps.set_params, (ps.num_cells, 1))
+            sim = lib.create(ps.nbr_offsets, ps.nbr_ids, cp, ps.set_params, ps.init_conc, 0.01)
+            chunks = sim.run(min(minutes, ps.duration), 1.0)
+            steps += chunks * 100 * ps.num_cells
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "unit": "cell-steps/s", "cores": 1,
+            "kind": "reference" if kinds == {"reference"} else "port",
+            "sample": "the first %d sets of each model of the mixed batch, %g min each, one host core, %.1f s"
+                      % (per_model, minutes, dt)}
+
+
+def run_mixed(a):
+    """The uneven mixed batch (her_model_2014 + Turing-Pattern) in one graph."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from dense_b200 import workloads
+    from dense_b200.autotune import Autotuner
+    from dense_b200.mixed import MixedBatch
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    num_sets = a.sets if a.sets != 4096 else 10000
+    groups = workloads.mixed_sets(num_sets, seed=3 + rank)
+    t0 = time.perf_counter()
+    tuner = Autotuner(device=local)
+    chosen = {m: tuner.tune(m, sets, 0.01) for m, sets in groups.items()}
+    tune_s = time.perf_counter() - t0
+    mb = MixedBatch(groups, 0.01, 1.0, device=local)
+    info = mb.info()
+    per_step = int(math.ceil(1200.0 / a.steps))  # chunks of 1 min
+    stream = torch.cuda.Stream()
+    for _ in range(a.warmup):
+        mb.run(per_step, stream=stream)
+    barrier()
+    mb.reset()
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    clocks = Clocks(local)
+    barrier()
+    ev[0].record(stream)
+    for k in range(a.steps):
+        mb.run(per_step, stream=stream)
+        ev[k + 1].record(stream)
+    stream.synchronize()
+    barrier()
+    clk = clocks.stop()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(a.steps)]
+    total_ms = ev[0].elapsed_time(ev[a.steps])
+    done = mb.done_cell_steps(100)
+    done_bytes = 0
+    for m, b in mb.batches.items():
+        chunks, _ = b.progress()
+        done_bytes += MIXED_BYTES[m] * int(sum(int(chunks[i]) * 100 * s.num_cells for i, s in enumerate(b.sets)))
+    status_bad = int(sum(int((b.status() != 0).sum()) for b in mb.batches.values()))
+    t = torch.tensor([total_ms, done], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
+    total_ms_max, all_done = float(t[0]), float(t[1])
+    value = all_done / (total_ms_max / 1e3)
+    mb.close()
+
+    # e2e: the batch built from host arrays, the whole horizon, every final state to the host
+    e2e_times, h2d, d2h = [], 0, 0
+    for k in range(a.e2e_steps):
+        barrier()
+        t1 = time.perf_counter()
+        m2 = MixedBatch(groups, 0.01, 1.0, device=local)
+        for b in m2.batches.values():
+            b.run(-1)
+        res = [b.state(i) for b in m2.batches.values() for i in range(len(b.sets))]
+        m2.close()
+        barrier()
+        e2e_times.append(time.perf_counter() - t1)
+        if k == 0:
+            h2d = sum(s.set_params.nbytes + s.nbr_offsets.nbytes + s.nbr_ids.nbytes for v in groups.values()
+                      for s in v)
+            d2h = sum(r.nbytes for r in res)
+    e2e_s = max(e2e_times) if e2e_times else float("nan")
+    if world > 1:
+        x = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(x[0])
+    hbm, peak_src = peaks()
+    achieved = done_bytes / (total_ms / 1e3) / 1e9
+    cpu = mixed_cpu_sample(groups) if (rank == 0 and world == 1 and not a.no_cpu) else None
+    if rank == 0:
+        from dense_b200.engine import plan
+        # one launch per kernel group of each engine (register kernel, one per memory-kernel CTA size)
+        n_launch = sum(len(set(plan(m, b.sets, 0.01, 1.0)[1].tolist())) for m, b in mb.batches.items())
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": total_ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": MIXED_WORKLOAD % num_sets,
+                       "sets": {m: len(v) for m, v in groups.items()},
+                       "step": "one graph replay advancing every unfinished set %d min" % per_step,
+                       "schedules": {m: {"%d,%d" % k: list(v) for k, v in c.items()} for m, c in chosen.items()},
+                       "autotune_s": tune_s,
+                       "l2": "inputs larger than L2 (%.0f MB of rings per GPU)" % (info["device_bytes"] / 1e6),
+                       "parallelism": "sets sharded across %d GPU(s), no exchange" % world},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None,
+                         "basis": "algorithmic bytes %d per her cell-step, %d per Turing cell-step; peak %s"
+                                  % (BYTES_PER_CELL_STEP, TURING_BYTES_PER_CELL_STEP, peak_src)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * info["total_cell_steps"] / e2e_s, "unit": "cell-steps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": a.e2e_steps,
+                    "what": "MixedBatch from host arrays + full horizons + every final state to host"},
+            "gpu_launches": a.steps * n_launch,
+            "clocks": clk,
+            "step_ms": {"min": min(step_ms), "max": max(step_ms)},
+            "status_nonzero_sets": status_bad,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def _ref_worker(args):
     seed, minutes = args
     r = cpu_sample("reference", num_sets=1, minutes=minutes, seed=seed)
@@ -188,9 +339,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--analyses", default="oscillation", choices=["oscillation", "none"],
                     help="the workload's analyses: Oscillation(mh1) every 0.1 min, or none")
+    ap.add_argument("--workload", default="batch", choices=["batch", "mixed"],
+                    help="batch: 4096 her_model_2014 sets of 200 cells; mixed: the uneven her + Turing batch "
+                         "(10000 sets unless --sets is given)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "mixed":
+        return run_mixed(a)
 
     import torch
     rank, world, local = dist_env()

@@ -866,7 +866,7 @@ int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D) {
 // Per-set device bytes and kernel of a batch, from the same planning as
 // dense_engine_create, without touching the GPU.
 int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_desc* in_sets, int64_t* set_bytes,
-                      int* set_kernel) {
+                      int* set_kernel, int* set_levels) {
   if (!run || num_sets <= 0 || !in_sets) return fail(DENSE_ERR_INVALID, "null argument or no sets");
   if (!(run->step_size > 0.0) || !(run->analysis_interval > 0.0))
     return fail(DENSE_ERR_INVALID, "step size and analysis interval must be positive");
@@ -893,6 +893,7 @@ int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_d
                      4 * (n + 1 + in.nbr_offsets[n] + static_cast<int64_t>(plan.lvl_off.size()) + n + 2) +
                      8 * (anl_block + NUM_SPECIES) + static_cast<int64_t>(sizeof(SetDesc) + sizeof(SetProgress));
     if (set_kernel) set_kernel[s] = plan.use_mem ? plan.mem_block : 0;
+    if (set_levels) set_levels[s] = plan.d.ordered ? static_cast<int>(plan.lvl_off.size()) - 1 : 1;
   }
   return DENSE_OK;
 }

@@ -64,7 +64,8 @@ _FUNCS = {
     "dense_model_reaction_name": (C.c_char_p, [C.c_int]),
     "dense_last_error": (C.c_char_p, []),
     "dense_engine_create": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_void_p)]),
-    "dense_engine_plan": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_int64), _I]),
+    "dense_engine_plan": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_int64), _I,
+                                    _I]),
     "dense_engine_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dense_engine_run_graph": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dense_engine_sync": (C.c_int, [C.c_void_p]),
@@ -220,17 +221,19 @@ def _describe(L, sets, analyses, step_size, analysis_interval, precision, device
 
 
 def plan(model, sets, step_size, analysis_interval, analyses=(), precision=FP64):
-    """Per-set device bytes and kernel (0 = register kernel, else the
-    memory-state kernel's CTA size) that a Batch of these sets would use;
-    needs no GPU."""
+    """Per-set device bytes, kernel (0 = register kernel, else the
+    memory-state kernel's CTA size) and dependency levels per step (1 unless
+    the set has ordered neighbour reads) that a Batch of these sets would
+    use; needs no GPU."""
     L = load(model) if isinstance(model, str) else model
     sets = list(sets)
     run, cset, keep = _describe(L, sets, list(analyses), step_size, analysis_interval, precision, 0)
     nbytes = np.zeros(len(sets), np.int64)
     kernel = np.zeros(len(sets), np.int32)
+    levels = np.zeros(len(sets), np.int32)
     L._check(L.lib.dense_engine_plan(C.byref(run), len(sets), cset, nbytes.ctypes.data_as(C.POINTER(C.c_int64)),
-                                     _ip(kernel)))
-    return nbytes, kernel
+                                     _ip(kernel), _ip(levels)))
+    return nbytes, kernel, levels
 
 
 class Batch:

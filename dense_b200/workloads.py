@@ -72,3 +72,47 @@ def cfg1_analyses(cells=200, interval=0.1):
 def batch_analyses(cells=200, interval=0.1):
     """Per-set oscillation period and amplitude of mh1 over every cell."""
     return [Analysis.oscillation(her_species("mh1"), 0, cells, 0.0, float("inf"), 4.0, interval)]
+
+
+def mixed_sets(num_sets, seed=3, her_fraction=0.5, lo=0.5, hi=2.0):
+    """The uneven mixed batch: `num_sets` sets split between her_model_2014
+    and Turing-Pattern (each set her with probability `her_fraction`).
+
+    * her_model_2014: cell count log-uniform over [16, 1024] in multiples of
+      4 on DENSE's default tissue of width 4 (``-c n -w 4``); every rate
+      scaled by exp(U(ln lo, ln hi)); every delay U[5, 20] min.
+    * Turing-Pattern: an N x N grid, N uniform in [8, 64] (``-c N*N -w N``);
+      every parameter scaled by exp(U(ln lo, ln hi)); the model's initial
+      concentrations.
+    * horizons U[100, 1200] min for both.
+
+    Returns {"her_model_2014": [ParameterSet], "turing": [ParameterSet]}.
+    """
+    from .engine import load
+    rng = np.random.Generator(np.random.PCG64(seed))
+    hp, tp = template_params("her_model_2014"), template_params("turing")
+    L = load("her_model_2014")
+    d0, d1 = L.num_reactions, L.num_reactions + L.num_delay_reactions
+    tinit = np.array(templates()["turing"]["init_conc"], np.float64)
+    graphs = {}
+
+    def graph(n, w):
+        if (n, w) not in graphs:
+            graphs[(n, w)] = default_graph(n, w)
+        return graphs[(n, w)]
+
+    out = {"her_model_2014": [], "turing": []}
+    for _ in range(num_sets):
+        horizon = float(rng.uniform(100.0, 1200.0))
+        if rng.random() < her_fraction:
+            n = 4 * int(round(np.exp(rng.uniform(np.log(4), np.log(256)))))
+            p = hp * np.exp(rng.uniform(np.log(lo), np.log(hi), size=hp.size))
+            p[d0:d1] = rng.uniform(5.0, 20.0, size=d1 - d0)
+            off, ids = graph(n, 4)
+            out["her_model_2014"].append(ParameterSet(off, ids, p, duration=horizon))
+        else:
+            N = int(rng.integers(8, 65))
+            p = tp * np.exp(rng.uniform(np.log(lo), np.log(hi), size=tp.size))
+            off, ids = graph(N * N, N)
+            out["turing"].append(ParameterSet(off, ids, p, init_conc=tinit, duration=horizon))
+    return out

@@ -191,10 +191,12 @@ DENSE_API int dense_engine_destroy(dense_engine* e);
    size themselves, sim/base.cpp:55-140): per set, the device bytes
    dense_engine_create would hold for it (set_bytes, or NULL) and the kernel
    it would run in (set_kernel: 0 = register kernel, else the memory-state
-   kernel's threads per CTA; or NULL).  Used to cut batches into waves that
-   fit the device. */
+   kernel's threads per CTA; or NULL) and the dependency levels of one of
+   its steps (set_levels: 1 unless neighbour reads see rows written in the
+   same step, DENSE's in-order cell loop; or NULL).  Used to size waves and
+   to bucket sets for schedule tuning. */
 DENSE_API int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_desc* sets,
-                                int64_t* set_bytes, int* set_kernel);
+                                int64_t* set_bytes, int* set_kernel, int* set_levels);
 
 /* No counterpart in DENSE: an addition of this library for callers that may
    not allocate device memory -- code running inside a framework that owns

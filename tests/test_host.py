@@ -91,16 +91,16 @@ def test_plan_kernels_and_bytes():
     off, ids = tissue.default_graph(200, 4)
     sets.append(ParameterSet(off, ids, p, duration=100, schedule=SCHEDULE_MEMORY))
     sets.append(ParameterSet(off, ids, p, duration=100, schedule=SCHEDULE_MEMORY, mem_block=96))
-    nbytes, kernel = plan("her_model_2014", sets, 0.01, 1.0)
-    assert list(kernel) == [0, 0, 256, 256, 224, 96]
+    nbytes, kernel, levels = plan("her_model_2014", sets, 0.01, 1.0)
+    assert list(kernel) == [0, 0, 256, 256, 224, 96] and (levels == 1).all()
     assert (np.diff(nbytes[:4]) > 0).all() and nbytes[4] == nbytes[5]
     tp = workloads.template_params("turing")
     ts = []
     for N in (8, 16, 64):
         off, ids = tissue.default_graph(N * N, N)
         ts.append(ParameterSet(off, ids, tp, duration=10))
-    _, kernel = plan("turing", ts, 0.01, 1.0)
-    assert list(kernel) == [32, 32, 32]
+    _, kernel, levels = plan("turing", ts, 0.01, 1.0)
+    assert list(kernel) == [32, 32, 32] and (levels > 1).all()
     with pytest.raises(DenseError):
         plan("her_model_2014", [ParameterSet(off, ids, tp, duration=10)], 0.01, 1.0)
     off, ids = tissue.default_graph(200, 4)
