@@ -35,7 +35,11 @@ def bucket_of(s, levels):
 
 
 def candidates(ordered, cells_log2, default_block):
-    """Schedules worth timing for a bucket: (schedule, mem_block) pairs."""
+    """Schedules worth timing for a bucket: (schedule, mem_block) pairs.
+    Ordered sets: the wave kernel with every row that fits in shared memory
+    or only the neighbour-read species there, or the memory kernel with
+    every row global; others: the register kernel (up to 256 cells) or the
+    memory kernel."""
     cells = 1 << cells_log2
     out = []
     if not ordered and cells <= 256:
@@ -45,6 +49,8 @@ def candidates(ordered, cells_log2, default_block):
         limit = default_block if ordered else max(32, cells)
         if b <= limit:
             out.append((E.SCHEDULE_MEMORY, b))
+    if ordered:
+        out += [(E.SCHEDULE_SHARED_NEIGHBOUR, default_block), (E.SCHEDULE_GLOBAL, default_block)]
     return out
 
 
@@ -119,14 +125,15 @@ class Autotuner:
                 sample = [sets[i] for i in pick]
                 default_block = int(max(kernel[i] for i in idx)) or 256
                 results = []
-                for cand in candidates(bucket[0], bucket[1], default_block):
+                cands = candidates(bucket[0], bucket[1], default_block)
+                for cand in cands if len(cands) > 1 else []:
                     v = time_schedule(model, sample, cand[0], cand[1], step_size, self.minutes,
                                       device=self.device)
                     results.append((v, cand))
                     self.log.append({"model": model, "bucket": bucket, "schedule": cand, "cell_steps_per_s": v})
                     if self.verbose:
                         print("autotune", model, bucket, cand, "%.3e" % v, flush=True)
-                chosen[bucket] = max(results)[1]
+                chosen[bucket] = max(results)[1] if results else cands[0]
                 self.cache[key] = list(chosen[bucket])
             for i in idx:
                 sets[i].schedule, sets[i].mem_block = chosen[bucket]

@@ -75,6 +75,7 @@ struct LagTracer {
   int* nbr_max;   // [NS] deepest neighbour lag, -1 none
   bool* ordered;  // a neighbour read of lag S-1
   bool* bad;
+  bool* ord_sp;   // [NS] species read by neighbours at lag S-1
   double getCon(specie_id sp) const { return conc[sp]; }
   double getCon(specie_id sp, int k) const {
     const int s = S[sp];
@@ -87,7 +88,7 @@ struct LagTracer {
     const int s = S[sp];
     if (k < 0 || k > s) *bad = true;
     const int lag = ((k % s) + s) % s;
-    if (lag == s - 1 && s > 1) *ordered = true;
+    if (lag == s - 1 && s > 1) *ordered = ord_sp[sp] = true;
     nbr_max[sp] = std::max(nbr_max[sp], lag);
     return nbr_value;
   }
@@ -99,7 +100,8 @@ struct LagTracer {
 struct SetPlan {
   SetDesc d;
   int status = 0;
-  bool use_mem = false;         // run by the memory-state kernel
+  bool use_mem = false;         // run by the memory-state kernel (or the wave kernel)
+  bool wave = false;            // an ordered set run by the wave kernel
   int mem_block = 256;          // its CTA size
   std::vector<int> lvl_off;     // memory kernel: level offsets into lvl_cells
   std::vector<int> lvl_cells;   // memory kernel: cells in level order
@@ -165,10 +167,12 @@ struct dense_engine {
   std::vector<AnalysisDesc> analyses;
   std::vector<int> init_status;
   DeviceBuffer d_sets, d_prog, d_params, d_nbr_off, d_nbr_idx, d_state, d_ring, d_anl, d_init_conc,
-      d_init_status, d_lists, d_lvl_off, d_lvl_cells;
+      d_init_status, d_lists, d_lvl_off, d_lvl_cells, d_wave_rec;
   int n_reg = 0, n_mem = 0;  // sets run by the register / memory kernels (d_lists: reg then mem)
-  // memory-kernel sets grouped by CTA size: (threads, first index in the mem list, count)
-  std::vector<std::array<int, 3>> mem_groups;
+  // memory- and wave-kernel sets in launch groups of one kernel, CTA size
+  // and dynamic shared memory: (wave, threads, shared bytes, first index in
+  // the mem list, count)
+  std::vector<std::array<int, 5>> mem_groups;
   std::map<int, cudaGraphExec_t> graphs;
   // the kernel launches of one run (register kernel, one per memory-kernel
   // group) fork onto side streams so that they run concurrently
@@ -210,7 +214,7 @@ int check_set(const dense_set_desc& in, const std::string& where) {
         return fail(DENSE_ERR_INVALID, where + "neighbour ids must ascend (DENSE keeps them in a std::set)");
     }
   }
-  if (in.schedule != DENSE_SCHEDULE_AUTO && in.schedule != DENSE_SCHEDULE_MEMORY)
+  if (in.schedule < DENSE_SCHEDULE_AUTO || in.schedule > DENSE_SCHEDULE_SHARED_NEIGHBOUR)
     return fail(DENSE_ERR_INVALID, where + "unknown schedule hint");
   if (in.mem_block != 0 && (in.mem_block < 32 || in.mem_block > 256 || in.mem_block % 32))
     return fail(DENSE_ERR_INVALID, where + "mem_block must be 32..256, a multiple of 32");
@@ -287,8 +291,8 @@ int build_analyses(const dense_run_desc* run, int num_sets, const dense_set_desc
   return DENSE_OK;
 }
 
-int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<double>& cell_params) {
-  const bool force_mem = in.schedule == DENSE_SCHEDULE_MEMORY;
+int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan, std::vector<double>& cell_params) {
+  const bool force_mem = in.schedule != DENSE_SCHEDULE_AUTO;
   const int n = in.num_cells;
   SetDesc& d = plan.d;
   d.n_cells = n;
@@ -331,6 +335,7 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
   int own_max[NUM_SPECIES], nbr_max[NUM_SPECIES];
   for (int sp = 0; sp < NUM_SPECIES; ++sp) { own_max[sp] = 0; nbr_max[sp] = -1; }
   bool ordered = false, bad = false;
+  bool ord_sp[NUM_SPECIES] = {};
   double prm[NUM_PARAMS];
   double conc[NUM_SPECIES];
   const double nbr_values[4] = {0.0, 2.0, 0.5, 7.25};
@@ -340,7 +345,7 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
     for (int i = 0; i < NUM_PARAMS; ++i) prm[i] = cell_params[static_cast<size_t>(i) * pcols + c];
     for (int pass = 0; pass < 4; ++pass) {
       for (int sp = 0; sp < NUM_SPECIES; ++sp) conc[sp] = pass == 0 ? 0.0 : (pass == 1 ? 1.0 : 0.37 * (sp + pass));
-      LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad};
+      LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad, ord_sp};
 #define REACTION(name) reaction<name>::active_rate(t);
 #include "reactions_list.hpp"
 #undef REACTION
@@ -353,6 +358,14 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
   d.ordered = ordered ? 1 : 0;
   plan.use_mem = ordered || n > kStepThreads || force_mem;
   plan_levels(in, ordered, plan);
+  // the wave kernel takes ordered sets whose cells have at most
+  // kWaveMaxNbrs neighbours and whose ids and level offsets fit 16 bits
+  if (ordered && in.schedule != DENSE_SCHEDULE_GLOBAL && n < 65536 &&
+      2 * static_cast<int64_t>(plan.lvl_off.size()) + 16 <= kWaveSmemBudget) {
+    plan.wave = true;
+    for (int c = 0; c < n; ++c)
+      if (in.nbr_offsets[c + 1] - in.nbr_offsets[c] > kWaveMaxNbrs) plan.wave = false;
+  }
   // memory-kernel CTA size: the hint, else the widest level in warps (32..256)
   int widest = 0;
   for (size_t l = 0; l + 1 < plan.lvl_off.size(); ++l) widest = std::max(widest, plan.lvl_off[l + 1] - plan.lvl_off[l]);
@@ -363,14 +376,55 @@ int plan_set(const dense_set_desc& in, double dt, SetPlan& plan, std::vector<dou
     if (own_max[sp] >= 1) depth = own_max[sp] + 1;
     if (nbr_max[sp] >= 0) depth = std::max(depth, nbr_max[sp] + 2);
     if (plan.use_mem) depth = std::max(depth, 2);
-    // a power of two, so a row is (step - lag) & (D - 1)
-    d.D[sp] = depth > 0 ? next_pow2(depth) : 0;
+    // a power of two, so a row is (step - lag) & (D - 1); the wave kernel
+    // indexes rows modulo D and keeps exactly the rows it reads
+    d.D[sp] = depth > 0 ? (plan.wave ? depth : next_pow2(depth)) : 0;
     depth = d.D[sp];
     d.ring_off[sp] = off;
     off += static_cast<int64_t>(depth) * n;
   }
+  // wave kernel shared memory, filled in priority order while it fits:
+  // the rows of the species read at lag S-1, the cell records, the rows of
+  // other neighbour-read species, then (unless the hint keeps them global)
+  // the rest; the 16-bit level offsets always, at the end
+  d.wave = plan.wave ? 1 : 0;
+  d.topo_off = -1;
+  d.lvl_smem_off = 0;
+  d.smem_bytes = 0;
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) d.smem_off[sp] = -1;
+  if (plan.wave) {
+    const int64_t lvl_bytes = (2 * static_cast<int64_t>(plan.lvl_off.size()) + 15) / 16 * 16;
+    int64_t used = 0;
+    auto take = [&](int64_t bytes) -> int64_t {
+      bytes = (bytes + 15) / 16 * 16;
+      if (used + bytes + lvl_bytes > kWaveSmemBudget) return -1;
+      const int64_t at = used;
+      used += bytes;
+      return at;
+    };
+    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+      if (ord_sp[sp]) d.smem_off[sp] = static_cast<int>(take(static_cast<int64_t>(d.D[sp]) * n * elem_bytes));
+    d.topo_off = static_cast<int>(take(16 * static_cast<int64_t>(n)));
+    for (int pass = 0; pass < 2; ++pass) {
+      if (pass == 1 && in.schedule == DENSE_SCHEDULE_SHARED_NEIGHBOUR) break;
+      for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        if (d.smem_off[sp] < 0 && (pass == 1 || nbr_max[sp] >= 0))
+          d.smem_off[sp] = static_cast<int>(take(static_cast<int64_t>(d.D[sp]) * n * elem_bytes));
+    }
+    d.lvl_smem_off = static_cast<int>(used);
+    d.smem_bytes = static_cast<int>(used + lvl_bytes);
+  }
   // chunk count: a = 0, 1, ... while a < duration / interval
   return DENSE_OK;
+}
+
+// Dynamic shared memory of a wave-kernel launch group holding a set that
+// needs `bytes`: a few fixed sizes, so sets of similar size share a launch.
+int wave_smem_bucket(int bytes) {
+  static const int kb[] = {8, 16, 24, 32, 48, 64, 80, 96, 112, 128, 160, 192};
+  for (int k : kb)
+    if (bytes <= k * 1024) return k * 1024;
+  return kWaveSmemBudget;
 }
 
 int64_t ring_elems(const SetDesc& d) {
@@ -430,7 +484,8 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   std::vector<int> off_all, idx_all;
   int64_t cells_total = 0, ring_total = 0;
   int max_cells = 0, max_edges = 0;
-  std::vector<int> reg_list, mem_list, mem_block_of, lvl_off_all, lvl_cells_all;
+  std::vector<int> reg_list, mem_list, mem_block_of, mem_smem_of, lvl_off_all, lvl_cells_all;
+  std::vector<uint16_t> rec_all;  // wave-kernel cell records, 8 x 16 bits each
   e->sets.resize(num_sets);
   e->init_status.resize(num_sets);
   std::vector<double> cp;
@@ -443,7 +498,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     }
     const int n = in.num_cells;
     SetPlan plan;
-    int rc = plan_set(in, dt, plan, cp);
+    int rc = plan_set(in, dt, run->precision == DENSE_FP64 ? 8 : 4, plan, cp);
     if (rc != DENSE_OK) return fail(rc, where + g_error);
     SetDesc& d = plan.d;
     const double chunks = in.duration / interval;  // run_simulation.hpp:127
@@ -471,6 +526,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     if (plan.use_mem) {
       mem_list.push_back(s);
       mem_block_of.push_back(plan.mem_block);
+      mem_smem_of.push_back(plan.wave ? wave_smem_bucket(d.smem_bytes) : -1);
       d.lvl_base = static_cast<int64_t>(lvl_off_all.size());
       lvl_off_all.insert(lvl_off_all.end(), plan.lvl_off.begin(), plan.lvl_off.end());
     } else {
@@ -479,6 +535,17 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       max_edges = std::max(max_edges, in.nbr_offsets[n]);
     }
     lvl_cells_all.insert(lvl_cells_all.end(), plan.lvl_cells.begin(), plan.lvl_cells.end());
+    if (plan.wave) {
+      // cell records in level order: {cell, neighbour count, ids (ascending), 0...}
+      d.rec_base = static_cast<int64_t>(rec_all.size() / 8);
+      for (int i = 0; i < n; ++i) {
+        const int c = plan.lvl_cells[i];
+        const int k0 = in.nbr_offsets[c], cnt = in.nbr_offsets[c + 1] - k0;
+        uint16_t r[8] = {static_cast<uint16_t>(c), static_cast<uint16_t>(cnt), 0, 0, 0, 0, 0, 0};
+        for (int e = 0; e < cnt; ++e) r[2 + e] = static_cast<uint16_t>(in.nbr_ids[k0 + e]);
+        rec_all.insert(rec_all.end(), r, r + 8);
+      }
+    }
     e->total_cell_steps += static_cast<int64_t>(n) * d.n_chunks * steps_per_chunk;
     e->sets[s] = d;
   }
@@ -500,6 +567,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   if ((rc = e->d_lists.alloc(sizeof(int) * num_sets))) return rc;
   if ((rc = e->d_lvl_off.alloc(sizeof(int) * std::max<size_t>(1, lvl_off_all.size())))) return rc;
   if ((rc = e->d_lvl_cells.alloc(sizeof(int) * lvl_cells_all.size()))) return rc;
+  if ((rc = e->d_wave_rec.alloc(sizeof(uint16_t) * rec_all.size()))) return rc;
   e->n_reg = static_cast<int>(reg_list.size());
   e->n_mem = static_cast<int>(mem_list.size());
   {
@@ -510,17 +578,20 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     };
     auto by_cost = [&](int x, int y) { return cost(x) != cost(y) ? cost(x) > cost(y) : x < y; };
     std::stable_sort(reg_list.begin(), reg_list.end(), by_cost);
-    // memory-kernel sets: grouped by CTA size, longest first in a group
-    std::vector<int> blk_of(num_sets, 0);
-    for (size_t k = 0; k < mem_list.size(); ++k) blk_of[mem_list[k]] = mem_block_of[k];
+    // memory- and wave-kernel sets: grouped by kernel, CTA size and shared
+    // memory bucket (-1: memory kernel), longest first in a group
+    std::vector<std::pair<int, int>> key_of(num_sets, {0, 0});
+    for (size_t k = 0; k < mem_list.size(); ++k) key_of[mem_list[k]] = {mem_smem_of[k], mem_block_of[k]};
     std::stable_sort(mem_list.begin(), mem_list.end(), [&](int x, int y) {
-      return blk_of[x] != blk_of[y] ? blk_of[x] < blk_of[y] : by_cost(x, y);
+      return key_of[x] != key_of[y] ? key_of[x] < key_of[y] : by_cost(x, y);
     });
     for (size_t k = 0; k < mem_list.size(); ++k) {
-      const int b = blk_of[mem_list[k]];
-      if (e->mem_groups.empty() || e->mem_groups.back()[0] != b)
-        e->mem_groups.push_back({b, static_cast<int>(k), 0});
-      e->mem_groups.back()[2]++;
+      const auto key = key_of[mem_list[k]];
+      const int wave = key.first >= 0 ? 1 : 0, smem = std::max(0, key.first);
+      if (e->mem_groups.empty() || e->mem_groups.back()[0] != wave || e->mem_groups.back()[1] != key.second ||
+          e->mem_groups.back()[2] != smem)
+        e->mem_groups.push_back({wave, key.second, smem, static_cast<int>(k), 0});
+      e->mem_groups.back()[4]++;
     }
     std::vector<int> lists(reg_list);
     lists.insert(lists.end(), mem_list.begin(), mem_list.end());
@@ -530,6 +601,9 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
                                cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaMemcpyAsync(e->d_lvl_cells.p, lvl_cells_all.data(), sizeof(int) * lvl_cells_all.size(),
                              cudaMemcpyHostToDevice, e->stream));
+    if (!rec_all.empty())
+      CUDA_TRY(cudaMemcpyAsync(e->d_wave_rec.p, rec_all.data(), sizeof(uint16_t) * rec_all.size(),
+                               cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
   }
   const int n_launch = (e->n_reg > 0 ? 1 : 0) + static_cast<int>(e->mem_groups.size());
@@ -574,6 +648,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   a.anl = static_cast<double*>(e->d_anl.p);
   a.lvl_off = static_cast<const int*>(e->d_lvl_off.p);
   a.lvl_cells = static_cast<const int*>(e->d_lvl_cells.p);
+  a.wave_rec = static_cast<const uint4*>(e->d_wave_rec.p);
   for (size_t i = 0; i < e->analyses.size(); ++i) a.analyses[i] = e->analyses[i];
   a.n_analyses = static_cast<int>(e->analyses.size());
   a.num_sets = num_sets;
@@ -655,8 +730,12 @@ static cudaError_t launch_all(dense_engine* e, const StepArgs& a, cudaStream_t s
   }
   for (const auto& g : e->mem_groups) {
     if ((r = stream_for(st)) != cudaSuccess) return r;
-    r = e->precision == DENSE_FP64 ? launch_step_mem_fp64(a, mem + g[1], g[2], g[0], st)
-                                   : launch_step_mem_fp32(a, mem + g[1], g[2], g[0], st);
+    if (g[0])
+      r = e->precision == DENSE_FP64 ? launch_step_wave_fp64(a, mem + g[3], g[4], g[1], g[2], st)
+                                     : launch_step_wave_fp32(a, mem + g[3], g[4], g[1], g[2], st);
+    else
+      r = e->precision == DENSE_FP64 ? launch_step_mem_fp64(a, mem + g[3], g[4], g[1], st)
+                                     : launch_step_mem_fp32(a, mem + g[3], g[4], g[1], st);
     if (r != cudaSuccess) return r;
     if ((r = join(st)) != cudaSuccess) return r;
   }
@@ -885,13 +964,15 @@ int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_d
     const std::string where = "set " + std::to_string(s) + ": ";
     if ((rc = check_set(in, where)) != DENSE_OK) return rc;
     SetPlan plan;
-    if ((rc = plan_set(in, run->step_size, plan, cp)) != DENSE_OK) return fail(rc, where + g_error);
+    if ((rc = plan_set(in, run->step_size, run->precision == DENSE_FP64 ? 8 : 4, plan, cp)) != DENSE_OK)
+      return fail(rc, where + g_error);
     const int64_t n = in.num_cells;
     if (set_bytes)
       set_bytes[s] = tsz * (((ring_elems(plan.d) + 31) & ~int64_t(31)) + 2 * NUM_SPECIES * n +
                             static_cast<int64_t>(cp.size())) +
                      4 * (n + 1 + in.nbr_offsets[n] + static_cast<int64_t>(plan.lvl_off.size()) + n + 2) +
-                     8 * (anl_block + NUM_SPECIES) + static_cast<int64_t>(sizeof(SetDesc) + sizeof(SetProgress));
+                     8 * (anl_block + NUM_SPECIES) + static_cast<int64_t>(sizeof(SetDesc) + sizeof(SetProgress)) +
+                     (plan.wave ? 16 * n : 0);
     if (set_kernel) set_kernel[s] = plan.use_mem ? plan.mem_block : 0;
     if (set_levels) set_levels[s] = plan.d.ordered ? static_cast<int>(plan.lvl_off.size()) - 1 : 1;
   }

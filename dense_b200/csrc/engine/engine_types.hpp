@@ -4,6 +4,8 @@
 #ifndef DENSE_B200_ENGINE_TYPES_HPP
 #define DENSE_B200_ENGINE_TYPES_HPP
 
+#include <vector_types.h>
+
 #include <cstdint>
 
 #include "dense_model_api.hpp"
@@ -78,7 +80,22 @@ struct SetDesc {
   int64_t lvl_base;      // memory kernel: offset of this set's level offsets (n_levels + 1)
   int n_levels;          // memory kernel: cell-dependency levels per step
   int ordered;           // neighbour reads of the row written in the same step (DENSE's cell order)
+  // wave kernel (ordered sets): rows indexed modulo D (not a power of two),
+  // cells as 16-byte records {cell, neighbour count, up to 6 neighbour ids}
+  // in level order
+  int wave;
+  int smem_off[kNS];     // byte offset of the species' rows in shared memory, -1: global
+  int lvl_smem_off;      // byte offset of the 16-bit level offsets in shared memory
+  int topo_off;          // byte offset of the records in shared memory, -1: global
+  int smem_bytes;        // dynamic shared memory the set needs
+  int64_t rec_base;      // first record of the set in StepArgs::wave_rec
 };
+
+// Dynamic shared memory a wave-kernel CTA may use (the 227 KB opt-in limit
+// of sm_100 less room for the kernel's static shared memory), and the
+// neighbours a wave-kernel cell record holds.
+constexpr int kWaveSmemBudget = 227 * 1024 - 8 * 1024;
+constexpr int kWaveMaxNbrs = 6;
 
 // Mutable per-set progress, updated by the kernels.
 struct SetProgress {
@@ -110,6 +127,7 @@ struct StepArgs {
   int uniform_params;       // every set has one parameter row for all its cells
   const int* lvl_off;       // memory kernel: per set, first index of each level in lvl_cells
   const int* lvl_cells;     // memory kernel: per set, its cells in level order
+  const uint4* wave_rec;    // wave kernel: per set, [n_cells] cell records in level order
   int n_vals;               // species the analyses observe (rows of the sampled-state buffer)
   int val_slot[kNS];        // row of each species in that buffer, -1 when no analysis observes it
 };

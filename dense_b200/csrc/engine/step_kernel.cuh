@@ -867,6 +867,347 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
   }
 }
 
+// ------------------------------------------------------------ wave kernel
+// Context of the wave kernel.  Rows are indexed modulo each species' row
+// count D (not a power of two: a species read by neighbours at lag S-1
+// keeps exactly S + 1 rows), from the lag-0 row r0 the kernel advances per
+// step; every species' rows sit behind a base pointer, in shared or global
+// memory; a cell's neighbour ids come from its 16-byte record.
+template <typename T, bool kUniform>
+struct WaveContext {
+  const T* cur;            // this cell's lag-0 state [NS] (registers)
+  const T* prm;            // parameters: shared row (pstride 1) or this cell's column (pstride n)
+  int pstride;
+  const int* S;            // DENSE ring sizes (registers)
+  const int* D;            // rows kept per species (registers)
+  const int* r0;           // row holding lag 0, per species (registers)
+  T* const* base;          // row 0 of each species, shared or global (registers)
+  T* const* wrow;          // the row this step writes, per species (registers)
+  const uint16_t* nbr;     // this cell's neighbour ids, ascending (registers)
+  int nnbr;
+  const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
+  const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
+  int n_cells;
+  int cell;
+  int* err;
+
+  __device__ __forceinline__ const T* row(specie_id sp, int lag) const {
+    const int r = r0[sp] - lag;
+    return base[sp] + (r < 0 ? r + D[sp] : r) * n_cells;
+  }
+
+  __device__ __forceinline__ T own(specie_id sp, int k) const {
+    const int s = S[sp];
+    int lag = k - 1;
+    if (lag < 0) lag += s;
+    if (static_cast<unsigned>(k) > static_cast<unsigned>(s)) {
+      if (k < 0 || k > s + 1) *err |= kSetBadDelay;
+      lag = ((k - 1) % s + s) % s;
+    }
+    if (lag == 0) return cur[sp];
+    if (lag >= D[sp]) {
+      *err |= kSetUnstagedLag;
+      return T(0);
+    }
+    return row(sp, lag)[cell];
+  }
+
+  __device__ __forceinline__ T own_lag(specie_id sp, int lag) const {
+    if (lag == 0) return cur[sp];
+    return row(sp, lag)[cell];
+  }
+
+  __device__ __forceinline__ T nbr_lag(specie_id sp, int lag) const {
+    const T* r = row(sp, lag);
+    T sum = T(0);
+#pragma unroll
+    for (int e = 0; e < kWaveMaxNbrs; ++e)
+      if (e < nnbr) sum += r[nbr[e]];
+    T avg = sum / static_cast<T>(nnbr);
+    return isnan(avg) ? T(0) : avg;
+  }
+
+  // Lag k mod S.  Lag S-1 is the row DENSE's cell-ordered loop is writing
+  // in this step: lower-numbered neighbours (all in lower levels) have
+  // their new value there, the others the value of S steps back.
+  __device__ __forceinline__ T nbr_avg(specie_id sp, int k) const {
+    const int s = S[sp];
+    int lag = k;
+    if (static_cast<unsigned>(k) >= static_cast<unsigned>(s)) {
+      if (k < 0 || k > s) *err |= kSetBadDelay;
+      lag = (k % s + s) % s;
+    }
+    if (lag == s - 1 && s > 1) {
+      if (D[sp] < s + 1) {
+        *err |= kSetOrderedReads;
+        return T(0);
+      }
+      const T* fresh = wrow[sp];
+      const T* old = row(sp, lag);
+      T sum = T(0);
+#pragma unroll
+      for (int e = 0; e < kWaveMaxNbrs; ++e) {
+        const int v = nbr[e];
+        if (e < nnbr) sum += (v < cell ? fresh : old)[v];
+      }
+      T avg = sum / static_cast<T>(nnbr);
+      return isnan(avg) ? T(0) : avg;
+    }
+    if (lag >= D[sp] - 1) {
+      *err |= kSetUnstagedLag;
+      return T(0);
+    }
+    return nbr_lag(sp, lag);
+  }
+
+  __device__ __forceinline__ T getCon(specie_id sp) const { return cur[sp]; }
+  __device__ __forceinline__ T getCon(specie_id sp, int k) const { return own(sp, k); }
+  __device__ __forceinline__ T getCon(specie_id sp, DelayArg<T> d) const {
+    if (kUniform) {
+      const int lag = olag[d.dr * kNS + sp];
+      if (lag >= 0) return own_lag(sp, lag);
+    }
+    return own(sp, d.k);
+  }
+  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, int k = 0) const { return nbr_avg(sp, k); }
+  __device__ __forceinline__ T calculateNeighborAvg(specie_id sp, DelayArg<T> d) const {
+    if (kUniform) {
+      const int lag = nlag[d.dr * kNS + sp];
+      if (lag >= 0) return nbr_lag(sp, lag);
+    }
+    return nbr_avg(sp, d.k);
+  }
+  __device__ __forceinline__ T getRate(reaction_id r) const { return prm[r * pstride]; }
+  __device__ __forceinline__ DelayArg<T> getDelay(delay_reaction_id d) const {
+    return DelayArg<T>{prm, pstride, static_cast<int>(d), static_cast<int>(prm[(kNR + d) * pstride])};
+  }
+  __device__ __forceinline__ T getCritVal(critspecie_id c) const { return prm[(kNR + kND + c) * pstride]; }
+};
+
+// The wave kernel: one CTA per ordered set (neighbour reads of the row
+// being written, as in DENSE's cell-ordered loop), one barrier per
+// dependency level, a thread per cell of a level.  The set's level offsets
+// and as many species' rows (and then its cell records) as fit stay in
+// shared memory for the whole launch: loaded from the set's history block
+// at entry, stored back at exit.  Records left in global memory are
+// fetched one level ahead.
+template <typename T, bool kKahan, bool kUniform>
+__global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs a, const int* set_list) {
+  extern __shared__ __align__(16) unsigned char w_dyn[];
+  __shared__ int s_S[kNS], s_D[kNS];
+  __shared__ T* s_base[kNS];
+  __shared__ T s_prm[kNP];
+  __shared__ int s_flags;
+  __shared__ double s_samples[kMaxAnalyses];
+  __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
+  __shared__ T* s_rows[kNS];
+
+  const int set = set_list[blockIdx.x];
+  const SetDesc& sd = a.sets[set];
+  const int n = sd.n_cells;
+  const int blk = blockDim.x;
+  const int tid = threadIdx.x;
+
+  const SetProgress pg = a.prog[set];
+  if ((pg.status & (kSetDropped | kSetNotRunnable)) || pg.finalized) return;
+
+  const int pstride = sd.param_stride;
+  const T* P = static_cast<const T*>(a.params) + sd.param_base;
+  T* ring = static_cast<T*>(a.ring) + sd.ring_base;
+  for (int i = tid; i < kNS; i += blk) {
+    s_S[i] = sd.S[i];
+    s_D[i] = sd.D[i];
+    s_base[i] = sd.smem_off[i] >= 0 ? reinterpret_cast<T*>(w_dyn + sd.smem_off[i]) : ring + sd.ring_off[i];
+  }
+  if (pstride == 0)
+    for (int i = tid; i < kNP; i += blk) s_prm[i] = P[i];
+  if (tid == 0) s_flags = 0;
+  double* anl = a.anl + sd.anl_base;
+  if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+
+  // level offsets (16-bit) and cell records: shared, or records global
+  const int n_levels = sd.n_levels;
+  uint16_t* t_lvl = reinterpret_cast<uint16_t*>(w_dyn + sd.lvl_smem_off);
+  {
+    const int* lvl_off = a.lvl_off + sd.lvl_base;
+    for (int i = tid; i <= n_levels; i += blk) t_lvl[i] = static_cast<uint16_t>(lvl_off[i]);
+  }
+  const uint4* g_rec = a.wave_rec + sd.rec_base;
+  const bool rec_shared = sd.topo_off >= 0;
+  const uint4* recs = rec_shared ? reinterpret_cast<const uint4*>(w_dyn + sd.topo_off) : g_rec;
+  if (rec_shared) {
+    uint4* dst = reinterpret_cast<uint4*>(w_dyn + sd.topo_off);
+    for (int i = tid; i < n; i += blk) dst[i] = g_rec[i];
+  }
+  for (int sp = 0; sp < kNS; ++sp) {
+    if (sd.smem_off[sp] < 0) continue;
+    T* dst = reinterpret_cast<T*>(w_dyn + sd.smem_off[sp]);
+    const T* src = ring + sd.ring_off[sp];
+    const int rows = sd.D[sp] * n;
+    for (int i = tid; i < rows; i += blk) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (kUniform) {
+    // the lag tables' bound checks take the row count as D - 1
+    for (int i = tid; i < kND * kNS; i += blk) {
+      const int d = i / kNS, sp = i % kNS;
+      const int k = static_cast<int>(s_prm[kNR + d]);
+      const int S = s_S[sp], m = s_D[sp] - 1;
+      int ol = -1, nl = -1;
+      if (k >= 0 && k <= S) {
+        ol = k - 1 < 0 ? S - 1 : k - 1;
+        if (ol != 0 && ol > m) ol = -1;
+        nl = k == S ? 0 : k;
+        if (nl >= m || nl == S - 1) nl = -1;
+      }
+      s_olag[i] = ol;
+      s_nlag[i] = nl;
+    }
+  }
+  __syncthreads();
+
+  T* comp_base = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS) + static_cast<int64_t>(kNS) * n;
+  int err = 0;
+  const T dt = static_cast<T>(a.dt);
+  int chunk = pg.chunk;
+  const int chunk_end = (a.chunk_count < 0 || sd.n_chunks - chunk < a.chunk_count)
+                            ? sd.n_chunks
+                            : chunk + a.chunk_count;
+  double age = pg.age;
+  int64_t step = pg.step;
+  bool dropped = false;
+  // per-set constants and per-step row pointers in registers
+  int lS[kNS], lD[kNS], r0[kNS];
+  T* lbase[kNS];
+  T* lcur[kNS];
+  T* lw[kNS];
+#pragma unroll
+  for (int sp = 0; sp < kNS; ++sp) {
+    lS[sp] = s_S[sp];
+    lD[sp] = s_D[sp];
+    lbase[sp] = s_base[sp];
+    r0[sp] = static_cast<int>(step % lD[sp]);
+  }
+
+  for (; chunk < chunk_end; ++chunk) {
+    if (a.n_analyses > 0) {
+      for (int i = tid; i < kNS; i += blk) {
+        const int row = a.val_slot[i];
+        if (row >= 0) s_rows[row] = s_base[i] + static_cast<int64_t>(step % s_D[i]) * n;
+      }
+      __syncthreads();
+      const bool bad = analyses_sample(a, anl, RingVals<T>{s_rows}, tid, tid, blk, n, age, s_samples);
+      if (bad) atomicOr(&s_flags, 1);
+      __syncthreads();
+      if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+      if (s_flags & 1) {
+        dropped = true;
+        break;
+      }
+    }
+    for (int s = 0; s < sd.steps_per_chunk; ++s) {
+      int rw[kNS];  // row this step writes
+#pragma unroll
+      for (int sp = 0; sp < kNS; ++sp) {
+        rw[sp] = r0[sp] + 1 == lD[sp] ? 0 : r0[sp] + 1;
+        lcur[sp] = lbase[sp] + r0[sp] * n;
+        lw[sp] = lbase[sp] + rw[sp] * n;
+      }
+      uint4 pre = make_uint4(0, 0, 0, 0);
+      if (!rec_shared && tid < t_lvl[1]) pre = recs[tid];
+      for (int l = 0; l < n_levels; ++l) {
+        const int i0 = t_lvl[l], i1 = t_lvl[l + 1];
+        uint4 here = pre;
+        if (!rec_shared && l + 1 < n_levels) {
+          // the next level's first record of this thread, fetched now
+          const int inext = i1 + tid;
+          if (inext < t_lvl[l + 2]) pre = recs[inext];
+        }
+        for (int i = i0 + tid; i < i1; i += blk) {
+          const uint4 raw = (rec_shared || i != i0 + tid) ? recs[i] : here;
+          const int cell = static_cast<int>(raw.x & 0xFFFFu);
+          const int cnt = static_cast<int>(raw.x >> 16);
+          const uint16_t nb[6] = {static_cast<uint16_t>(raw.y & 0xFFFFu), static_cast<uint16_t>(raw.y >> 16),
+                                  static_cast<uint16_t>(raw.z & 0xFFFFu), static_cast<uint16_t>(raw.z >> 16),
+                                  static_cast<uint16_t>(raw.w & 0xFFFFu), static_cast<uint16_t>(raw.w >> 16)};
+          T cur[kNS];
+#pragma unroll
+          for (int sp = 0; sp < kNS; ++sp) cur[sp] = lcur[sp][cell];
+          const T* prm = pstride == 0 ? s_prm : P + cell;
+          const int ps = pstride == 0 ? 1 : n;
+          WaveContext<T, kUniform> ctx{cur, prm, ps, lS, lD, r0, lbase, lw, nb, cnt, s_olag, s_nlag, n, cell, &err};
+          T dsp[kNS];
+#pragma unroll
+          for (int sp = 0; sp < kNS; ++sp) dsp[sp] = T(0);
+#define REACTION(name)                                                        \
+  {                                                                           \
+    const T rate_ = reaction<name>::active_rate(ctx);                         \
+    _Pragma("unroll") for (int j = 0; j < num_deltas_##name; j++)             \
+        dsp[delta_ids_##name[j]] += rate_ * static_cast<T>(deltas_##name[j]); \
+  }
+#include "reactions_list.hpp"
+#undef REACTION
+#pragma unroll
+          for (int sp = 0; sp < kNS; ++sp) {
+            T nxt;
+            if (kKahan) {
+              T& cp = comp_base[static_cast<int64_t>(sp) * n + cell];
+              const T y = dt * dsp[sp] - cp;
+              const T t = cur[sp] + y;
+              cp = (t - cur[sp]) - y;
+              nxt = t;
+            } else {
+              nxt = cur[sp] + dt * dsp[sp];
+            }
+            lw[sp][cell] = nxt;
+          }
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int sp = 0; sp < kNS; ++sp) r0[sp] = rw[sp];
+      ++step;
+    }
+    age += a.interval;
+  }
+
+  // lag-0 state to the state block (what read_state returns), shared rows
+  // back to the history block
+  T* state = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS);
+  for (int i = tid; i < kNS * n; i += blk) {
+    const int sp = i / n, cell = i % n;
+    state[i] = s_base[sp][static_cast<int64_t>(step % s_D[sp]) * n + cell];
+  }
+  for (int sp = 0; sp < kNS; ++sp) {
+    if (sd.smem_off[sp] < 0) continue;
+    const T* src = reinterpret_cast<const T*>(w_dyn + sd.smem_off[sp]);
+    T* dst = ring + sd.ring_off[sp];
+    const int rows = sd.D[sp] * n;
+    for (int i = tid; i < rows; i += blk) dst[i] = src[i];
+  }
+  if (err) atomicOr(&s_flags, err << 1);
+  if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+  __syncthreads();
+  const int status = pg.status | (dropped ? kSetDropped : 0) | (s_flags >> 1);
+  const bool finish = !dropped && chunk >= sd.n_chunks;
+  if (finish) {
+    for (int ai = 0; ai < a.n_analyses; ++ai) {
+      const AnalysisDesc& A = a.analyses[ai];
+      if (A.kind == kOscillation)
+        for (int c = tid; c < n; c += blk) osc_cell_finalize(anl + A.off, A, c, s_samples[ai]);
+    }
+  }
+  if (tid == 0) {
+    SetProgress out = pg;
+    out.step = step;
+    out.chunk = chunk;
+    out.age = age;
+    out.status = status;
+    out.finalized = finish ? 1 : 0;
+    a.prog[set] = out;
+  }
+}
+
 // Fills every set's state, history rows and analysis state with their
 // initial values: all rows of every ring hold the initial concentrations
 // (determ.cpp:42-51, zeros when none are given), Basic minima start at
@@ -959,6 +1300,23 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
       dense_step_mem_kernel<T, KAHAN, true><<<n_sets, block, 0, s>>>(a, set_list);               \
     else                                                                                        \
       dense_step_mem_kernel<T, KAHAN, false><<<n_sets, block, 0, s>>>(a, set_list);              \
+    return cudaGetLastError();                                                                  \
+  }                                                                                             \
+  cudaError_t launch_step_wave_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets,      \
+                                        int block, int smem, cudaStream_t s) {                  \
+    if (n_sets <= 0) return cudaSuccess;                                                        \
+    cudaError_t e;                                                                              \
+    if (a.uniform_params) {                                                                     \
+      e = cudaFuncSetAttribute(dense_step_wave_kernel<T, KAHAN, true>,                          \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, kWaveSmemBudget);              \
+      if (e != cudaSuccess) return e;                                                           \
+      dense_step_wave_kernel<T, KAHAN, true><<<n_sets, block, smem, s>>>(a, set_list);          \
+    } else {                                                                                    \
+      e = cudaFuncSetAttribute(dense_step_wave_kernel<T, KAHAN, false>,                         \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, kWaveSmemBudget);              \
+      if (e != cudaSuccess) return e;                                                           \
+      dense_step_wave_kernel<T, KAHAN, false><<<n_sets, block, smem, s>>>(a, set_list);         \
+    }                                                                                           \
     return cudaGetLastError();                                                                  \
   }                                                                                             \
   cudaError_t launch_step_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets, size_t smem, \

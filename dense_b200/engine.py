@@ -30,6 +30,8 @@ SET_BAD_DELAY = 8
 SET_ORDERED_READS = 16
 SCHEDULE_AUTO = 0
 SCHEDULE_MEMORY = 1
+SCHEDULE_GLOBAL = 2
+SCHEDULE_SHARED_NEIGHBOUR = 3
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)

@@ -63,8 +63,11 @@ extern "C" {
 #define DENSE_SET_ORDERED_READS 16 /* neighbour reads of rows written in the same step */
 
 /* schedule hint of a set (dense_set_desc.schedule) */
-#define DENSE_SCHEDULE_AUTO 0    /* register kernel when the set fits one, else memory kernel */
-#define DENSE_SCHEDULE_MEMORY 1  /* memory-state kernel */
+#define DENSE_SCHEDULE_AUTO 0              /* register kernel when the set fits one, else memory kernel */
+#define DENSE_SCHEDULE_MEMORY 1            /* memory-state kernel; sets with in-order neighbour reads in
+                                              the wave kernel, rows in shared memory as far as they fit */
+#define DENSE_SCHEDULE_GLOBAL 2            /* memory-state kernel with every row in global memory */
+#define DENSE_SCHEDULE_SHARED_NEIGHBOUR 3  /* as MEMORY, but only neighbour-read species in shared memory */
 
 /* arithmetic of a batch */
 #define DENSE_FP64 0        /* matches DENSE's CPU path bit for bit */

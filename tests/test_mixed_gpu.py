@@ -43,18 +43,25 @@ def test_her_every_schedule_bitwise(cells, width, hints):
     _assert_same(_oracle_vs_engine("her_model_2014", spec, 0.01, 0.1, an), an)
 
 
-@pytest.mark.parametrize("grid,blocks", [(12, [0, 32, 64]), (37, [0, 32, 64, 256])])
-def test_turing_every_schedule_bitwise(grid, blocks):
-    """Turing's ordered neighbour reads under memory-kernel CTAs of several
-    widths (one warp per set up to idle lanes)."""
+TURING_HINTS = [(0, 0), (1, 32), (1, 64), (E.SCHEDULE_GLOBAL, 0), (E.SCHEDULE_SHARED_NEIGHBOUR, 0),
+                (E.SCHEDULE_GLOBAL, 64)]
+
+
+@pytest.mark.parametrize("grid,minutes", [(12, 3.0), (37, 3.0), (64, 0.5)])
+def test_turing_every_schedule_bitwise(grid, minutes):
+    """Turing's ordered neighbour reads in the wave kernel (rows in shared
+    memory as far as they fit: all species at 12 x 12, the in-order species
+    and records at 37 x 37, only the in-order species at 64 x 64), with
+    only neighbour-read species shared, and in the memory kernel with every
+    row global; CTAs of one and two warps."""
     p = workloads.template_params("turing")
     ic = np.array(workloads.templates()["turing"]["init_conc"])
     off, ids = default_graph(grid * grid, grid)
     spec = []
-    for b in blocks:
-        spec.append((E.ParameterSet(off, ids, p, init_conc=ic, duration=3.0, schedule=1 if b else 0,
-                                    mem_block=b), np.tile(p, (grid * grid, 1))))
-    an = [E.Analysis.basic([0, 1, 2, 3], 0, 144)]
+    for sched, b in TURING_HINTS:
+        spec.append((E.ParameterSet(off, ids, p, init_conc=ic, duration=minutes, schedule=sched, mem_block=b),
+                     np.tile(p, (grid * grid, 1))))
+    an = [E.Analysis.basic([0, 1, 2, 3], 0, 144), E.Analysis.oscillation([1], 0, 144, 0.0, float("inf"), 0.2, 0.1)]
     _assert_same(_oracle_vs_engine("turing", spec, 0.01, 0.1, an), an)
 
 
@@ -88,7 +95,7 @@ def test_mixed_graph_matches_plain_runs_and_autotune():
     tuner = Autotuner(sample_sets=2, minutes=0.2)
     for m, sets in tuned.items():
         chosen = tuner.tune(m, sets, 0.01)
-        assert chosen and all(s.schedule in (0, 1) for s in sets)
+        assert chosen and all(s.schedule in (0, 1, 2, 3) for s in sets)
     mb = MixedBatch(tuned, 0.01, 0.1)
     for _ in range(7):  # 7 x 9 chunks cover the 6-minute horizons
         mb.run(9)
