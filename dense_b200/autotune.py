@@ -36,10 +36,9 @@ def bucket_of(s, levels):
 
 def candidates(ordered, cells_log2, default_block):
     """Schedules worth timing for a bucket: (schedule, mem_block) pairs.
-    Ordered sets: the wave kernel with every row that fits in shared memory
-    or only the neighbour-read species there, or the memory kernel with
-    every row global; others: the register kernel (up to 256 cells) or the
-    memory kernel."""
+    Ordered sets: the wave kernel with every row that fits in shared memory,
+    only the neighbour-read species there, or every row in global memory;
+    others: the register kernel (up to 256 cells) or the memory kernel."""
     cells = 1 << cells_log2
     out = []
     if not ordered and cells <= 256:
@@ -50,7 +49,9 @@ def candidates(ordered, cells_log2, default_block):
         if b <= limit:
             out.append((E.SCHEDULE_MEMORY, b))
     if ordered:
-        out += [(E.SCHEDULE_SHARED_NEIGHBOUR, default_block), (E.SCHEDULE_GLOBAL, default_block)]
+        out.append((E.SCHEDULE_SHARED_NEIGHBOUR, default_block))
+        # every row global: more sets per SM, longer levels
+        out.append((E.SCHEDULE_WAVE_GLOBAL, default_block))
     return out
 
 

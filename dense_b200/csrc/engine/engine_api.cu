@@ -170,12 +170,16 @@ struct dense_engine {
       d_init_status, d_lists, d_lvl_off, d_lvl_cells, d_wave_rec;
   int n_reg = 0, n_mem = 0;  // sets run by the register / memory kernels (d_lists: reg then mem)
   // memory- and wave-kernel sets in launch groups of one kernel, CTA size
-  // and dynamic shared memory: (wave, threads, shared bytes, first index in
-  // the mem list, count)
+  // and dynamic shared memory: (kernel: 0 memory, 1 wave, 2 wave with
+  // everything shared; threads; shared bytes; first index in the mem list;
+  // count)
   std::vector<std::array<int, 5>> mem_groups;
   std::map<int, cudaGraphExec_t> graphs;
-  // the kernel launches of one run (register kernel, one per memory-kernel
-  // group) fork onto side streams so that they run concurrently
+  // the kernel launches of one run (register kernel, one per memory- or
+  // wave-kernel group) fork onto side streams of their own so that they run
+  // concurrently; launch k goes to side[k], whose priority ranks the
+  // group's longest set (the block scheduler starts the CTAs of
+  // higher-priority streams first)
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev_join;
   cudaEvent_t ev_fork = nullptr;
@@ -214,7 +218,7 @@ int check_set(const dense_set_desc& in, const std::string& where) {
         return fail(DENSE_ERR_INVALID, where + "neighbour ids must ascend (DENSE keeps them in a std::set)");
     }
   }
-  if (in.schedule < DENSE_SCHEDULE_AUTO || in.schedule > DENSE_SCHEDULE_SHARED_NEIGHBOUR)
+  if (in.schedule < DENSE_SCHEDULE_AUTO || in.schedule > DENSE_SCHEDULE_WAVE_GLOBAL)
     return fail(DENSE_ERR_INVALID, where + "unknown schedule hint");
   if (in.mem_block != 0 && (in.mem_block < 32 || in.mem_block > 256 || in.mem_block % 32))
     return fail(DENSE_ERR_INVALID, where + "mem_block must be 32..256, a multiple of 32");
@@ -402,10 +406,11 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
       used += bytes;
       return at;
     };
-    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+    const bool global_rows = in.schedule == DENSE_SCHEDULE_WAVE_GLOBAL;
+    for (int sp = 0; sp < NUM_SPECIES && !global_rows; ++sp)
       if (ord_sp[sp]) d.smem_off[sp] = static_cast<int>(take(static_cast<int64_t>(d.D[sp]) * n * elem_bytes));
-    d.topo_off = static_cast<int>(take(16 * static_cast<int64_t>(n)));
-    for (int pass = 0; pass < 2; ++pass) {
+    d.topo_off = global_rows ? -1 : static_cast<int>(take(16 * static_cast<int64_t>(n)));
+    for (int pass = 0; pass < 2 && !global_rows; ++pass) {
       if (pass == 1 && in.schedule == DENSE_SCHEDULE_SHARED_NEIGHBOUR) break;
       for (int sp = 0; sp < NUM_SPECIES; ++sp)
         if (d.smem_off[sp] < 0 && (pass == 1 || nbr_max[sp] >= 0))
@@ -421,7 +426,7 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
 // Dynamic shared memory of a wave-kernel launch group holding a set that
 // needs `bytes`: a few fixed sizes, so sets of similar size share a launch.
 int wave_smem_bucket(int bytes) {
-  static const int kb[] = {8, 16, 24, 32, 48, 64, 80, 96, 112, 128, 160, 192};
+  static const int kb[] = {1, 2, 4, 8, 16, 24, 32, 48, 64, 80, 96, 112, 128, 160, 192};
   for (int k : kb)
     if (bytes <= k * 1024) return k * 1024;
   return kWaveSmemBudget;
@@ -484,7 +489,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
   std::vector<int> off_all, idx_all;
   int64_t cells_total = 0, ring_total = 0;
   int max_cells = 0, max_edges = 0;
-  std::vector<int> reg_list, mem_list, mem_block_of, mem_smem_of, lvl_off_all, lvl_cells_all;
+  std::vector<int> reg_list, mem_list, mem_block_of, mem_smem_of, mem_kind_of, lvl_off_all, lvl_cells_all;
   std::vector<uint16_t> rec_all;  // wave-kernel cell records, 8 x 16 bits each
   e->sets.resize(num_sets);
   e->init_status.resize(num_sets);
@@ -527,6 +532,9 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       mem_list.push_back(s);
       mem_block_of.push_back(plan.mem_block);
       mem_smem_of.push_back(plan.wave ? wave_smem_bucket(d.smem_bytes) : -1);
+      bool all_shared = plan.wave && d.topo_off >= 0;
+      for (int sp = 0; sp < NUM_SPECIES; ++sp) all_shared = all_shared && d.smem_off[sp] >= 0;
+      mem_kind_of.push_back(plan.wave ? (all_shared ? 2 : 1) : 0);
       d.lvl_base = static_cast<int64_t>(lvl_off_all.size());
       lvl_off_all.insert(lvl_off_all.end(), plan.lvl_off.begin(), plan.lvl_off.end());
     } else {
@@ -580,17 +588,19 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     std::stable_sort(reg_list.begin(), reg_list.end(), by_cost);
     // memory- and wave-kernel sets: grouped by kernel, CTA size and shared
     // memory bucket (-1: memory kernel), longest first in a group
-    std::vector<std::pair<int, int>> key_of(num_sets, {0, 0});
-    for (size_t k = 0; k < mem_list.size(); ++k) key_of[mem_list[k]] = {mem_smem_of[k], mem_block_of[k]};
+    // key: (kernel: 0 memory, 1 wave, 2 wave with everything shared; shared
+    // memory bucket; CTA size)
+    std::vector<std::array<int, 3>> key_of(num_sets, {0, 0, 0});
+    for (size_t k = 0; k < mem_list.size(); ++k)
+      key_of[mem_list[k]] = {mem_kind_of[k], std::max(0, mem_smem_of[k]), mem_block_of[k]};
     std::stable_sort(mem_list.begin(), mem_list.end(), [&](int x, int y) {
       return key_of[x] != key_of[y] ? key_of[x] < key_of[y] : by_cost(x, y);
     });
     for (size_t k = 0; k < mem_list.size(); ++k) {
       const auto key = key_of[mem_list[k]];
-      const int wave = key.first >= 0 ? 1 : 0, smem = std::max(0, key.first);
-      if (e->mem_groups.empty() || e->mem_groups.back()[0] != wave || e->mem_groups.back()[1] != key.second ||
-          e->mem_groups.back()[2] != smem)
-        e->mem_groups.push_back({wave, key.second, smem, static_cast<int>(k), 0});
+      if (e->mem_groups.empty() || e->mem_groups.back()[0] != key[0] || e->mem_groups.back()[1] != key[2] ||
+          e->mem_groups.back()[2] != key[1])
+        e->mem_groups.push_back({key[0], key[2], key[1], static_cast<int>(k), 0});
       e->mem_groups.back()[4]++;
     }
     std::vector<int> lists(reg_list);
@@ -606,13 +616,39 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
                                cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
   }
-  const int n_launch = (e->n_reg > 0 ? 1 : 0) + static_cast<int>(e->mem_groups.size());
-  if (n_launch > 1) {
+  {
+    // one side stream per launch, prioritised by the group's longest set in
+    // dependent steps: Euler steps x levels (x cells per thread for the
+    // memory kernel); register-kernel sets count one level per step
+    std::vector<std::pair<double, int>> est;  // (latency estimate, launch index)
+    int k = 0;
+    if (e->n_reg > 0) {
+      double m = 0;
+      for (int i : reg_list) m = std::max(m, static_cast<double>(e->sets[i].n_chunks) * e->sets[i].steps_per_chunk);
+      est.push_back({m, k++});
+    }
+    for (const auto& g : e->mem_groups) {
+      double m = 0;
+      for (int j = g[3]; j < g[3] + g[4]; ++j) {
+        const SetDesc& d = e->sets[mem_list[j]];
+        const double per_step = g[0] ? d.n_levels : d.n_levels * std::ceil(static_cast<double>(d.n_cells) /
+                                                                            (d.n_levels * g[1]));
+        m = std::max(m, static_cast<double>(d.n_chunks) * d.steps_per_chunk * per_step);
+      }
+      est.push_back({m, k++});
+    }
+    std::stable_sort(est.begin(), est.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+      return x.first > y.first;
+    });
+    int least = 0, greatest = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    std::vector<int> prio(est.size(), least);
+    for (size_t r = 0; r < est.size(); ++r) prio[est[r].second] = std::min(least, greatest + static_cast<int>(r));
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
-    for (int i = 1; i < n_launch; ++i) {
+    for (size_t i = 0; i < est.size(); ++i) {
       cudaStream_t x;
       cudaEvent_t ev;
-      CUDA_TRY(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      CUDA_TRY(cudaStreamCreateWithPriority(&x, cudaStreamNonBlocking, prio[i]));
       e->side.push_back(x);
       CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
       e->ev_join.push_back(ev);
@@ -695,28 +731,24 @@ int dense_engine_reset(dense_engine* e, void* stream) {
   return DENSE_OK;
 }
 
-// One run: the register kernel over its sets, and the memory kernel once
-// per CTA-size group.  With more than one launch, every launch after the
-// first goes to a side stream forked from `s` and joined back into it, so
-// the kernels share the GPU instead of running one after the other (in a
-// captured graph they become parallel branches).
+// One run: the register kernel over its sets, the memory or wave kernel
+// once per group.  Every launch goes to its own side stream forked from `s`
+// and joined back into it, so the kernels share the GPU instead of running
+// one after the other (in a captured graph they become parallel branches
+// that keep their priorities).
 static cudaError_t launch_all(dense_engine* e, const StepArgs& a, cudaStream_t s) {
   const int* reg = static_cast<const int*>(e->d_lists.p);
   const int* mem = reg + e->n_reg;
-  const bool fork = !e->side.empty();
   cudaError_t r;
-  if (fork && (r = cudaEventRecord(e->ev_fork, s)) != cudaSuccess) return r;
+  if ((r = cudaEventRecord(e->ev_fork, s)) != cudaSuccess) return r;
   int k = 0;  // launches issued so far
   auto stream_for = [&](cudaStream_t& st) -> cudaError_t {
-    st = (fork && k > 0) ? e->side[k - 1] : s;
-    return st != s ? cudaStreamWaitEvent(st, e->ev_fork, 0) : cudaSuccess;
+    st = e->side[k];
+    return cudaStreamWaitEvent(st, e->ev_fork, 0);
   };
   auto join = [&](cudaStream_t st) -> cudaError_t {
-    cudaError_t rj = cudaSuccess;
-    if (st != s) {
-      rj = cudaEventRecord(e->ev_join[k - 1], st);
-      if (rj == cudaSuccess) rj = cudaStreamWaitEvent(s, e->ev_join[k - 1], 0);
-    }
+    cudaError_t rj = cudaEventRecord(e->ev_join[k], st);
+    if (rj == cudaSuccess) rj = cudaStreamWaitEvent(s, e->ev_join[k], 0);
     ++k;
     return rj;
   };
@@ -731,8 +763,8 @@ static cudaError_t launch_all(dense_engine* e, const StepArgs& a, cudaStream_t s
   for (const auto& g : e->mem_groups) {
     if ((r = stream_for(st)) != cudaSuccess) return r;
     if (g[0])
-      r = e->precision == DENSE_FP64 ? launch_step_wave_fp64(a, mem + g[3], g[4], g[1], g[2], st)
-                                     : launch_step_wave_fp32(a, mem + g[3], g[4], g[1], g[2], st);
+      r = e->precision == DENSE_FP64 ? launch_step_wave_fp64(a, mem + g[3], g[4], g[1], g[2], g[0] == 2, st)
+                                     : launch_step_wave_fp32(a, mem + g[3], g[4], g[1], g[2], g[0] == 2, st);
     else
       r = e->precision == DENSE_FP64 ? launch_step_mem_fp64(a, mem + g[3], g[4], g[1], st)
                                      : launch_step_mem_fp32(a, mem + g[3], g[4], g[1], st);
@@ -774,7 +806,7 @@ int dense_engine_run_graph(dense_engine* e, int num_chunks, void* stream) {
     CUDA_TRY(le);
     CUDA_TRY(ce);
     cudaGraphExec_t ge;
-    cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    cudaError_t ie = cudaGraphInstantiateWithFlags(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     CUDA_TRY(ie);
     it = e->graphs.emplace(num_chunks, ge).first;
@@ -976,6 +1008,62 @@ int dense_engine_plan(const dense_run_desc* run, int num_sets, const dense_set_d
     if (set_kernel) set_kernel[s] = plan.use_mem ? plan.mem_block : 0;
     if (set_levels) set_levels[s] = plan.d.ordered ? static_cast<int>(plan.lvl_off.size()) - 1 : 1;
   }
+  return DENSE_OK;
+}
+
+// One CUDA graph over several engines (of any models' libraries): each
+// engine's dense_engine_run, passed as a function pointer, is captured on a
+// stream of its own forked from the capture stream, and the graph keeps
+// every kernel node's stream priority.
+int dense_graph_capture(int num_engines, void* const* run_fns, dense_engine* const* engines, int num_chunks,
+                        int device, void** graph_exec) {
+  if (num_engines <= 0 || !run_fns || !engines || !graph_exec) return fail(DENSE_ERR_INVALID, "null argument");
+  *graph_exec = nullptr;
+  CUDA_TRY(cudaSetDevice(device));
+  typedef int (*run_fn)(dense_engine*, int, void*);
+  cudaStream_t cap;
+  CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  std::vector<cudaStream_t> st(num_engines, nullptr);
+  std::vector<cudaEvent_t> ev(num_engines + 1, nullptr);
+  cudaError_t ce = cudaSuccess;
+  for (int i = 0; i < num_engines && ce == cudaSuccess; ++i) ce = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
+  for (int i = 0; i <= num_engines && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+  int rc = DENSE_OK;
+  cudaGraph_t g = nullptr;
+  if (ce == cudaSuccess) ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    cudaError_t le = cudaEventRecord(ev[num_engines], cap);
+    for (int i = 0; i < num_engines && le == cudaSuccess && rc == DENSE_OK; ++i) {
+      le = cudaStreamWaitEvent(st[i], ev[num_engines], 0);
+      if (le == cudaSuccess) rc = reinterpret_cast<run_fn>(run_fns[i])(engines[i], num_chunks, st[i]);
+      if (le == cudaSuccess && rc == DENSE_OK) le = cudaEventRecord(ev[i], st[i]);
+      if (le == cudaSuccess && rc == DENSE_OK) le = cudaStreamWaitEvent(cap, ev[i], 0);
+    }
+    ce = cudaStreamEndCapture(cap, &g);
+    if (le != cudaSuccess) ce = le;
+  }
+  cudaGraphExec_t ge = nullptr;
+  if (ce == cudaSuccess && rc == DENSE_OK) ce = cudaGraphInstantiateWithFlags(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
+  if (g) cudaGraphDestroy(g);
+  for (auto x : st)
+    if (x) cudaStreamDestroy(x);
+  for (auto x : ev)
+    if (x) cudaEventDestroy(x);
+  cudaStreamDestroy(cap);
+  if (rc != DENSE_OK) return fail(rc, "capture: " + g_error);
+  if (ce != cudaSuccess) return fail(DENSE_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+  *graph_exec = ge;
+  return DENSE_OK;
+}
+
+int dense_graph_launch(void* graph_exec, void* stream) {
+  if (!graph_exec) return fail(DENSE_ERR_INVALID, "null graph");
+  CUDA_TRY(cudaGraphLaunch(static_cast<cudaGraphExec_t>(graph_exec), static_cast<cudaStream_t>(stream)));
+  return DENSE_OK;
+}
+
+int dense_graph_destroy(void* graph_exec) {
+  if (graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph_exec));
   return DENSE_OK;
 }
 

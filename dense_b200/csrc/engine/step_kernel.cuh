@@ -25,6 +25,7 @@
 
 #include <cuda_runtime.h>
 
+#include "count_div.cuh"
 #include "engine_types.hpp"
 
 namespace dense_b200 {
@@ -885,19 +886,31 @@ struct WaveContext {
   T* const* wrow;          // the row this step writes, per species (registers)
   const uint16_t* nbr;     // this cell's neighbour ids, ascending (registers)
   int nnbr;
+  T rc;                    // RN(1 / nnbr)
   const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
   const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
   int n_cells;
   int cell;
   int* err;
 
+  // DENSE's ring size: max delay / dt + 2, so 2 for every species of a
+  // model without delay reactions
+  __device__ __forceinline__ int ring_size(specie_id sp) const { return kND == 0 ? 2 : S[sp]; }
+
   __device__ __forceinline__ const T* row(specie_id sp, int lag) const {
     const int r = r0[sp] - lag;
     return base[sp] + (r < 0 ? r + D[sp] : r) * n_cells;
   }
 
+  __device__ __forceinline__ T average(T sum) const {
+    const T avg = div_by_count(sum, static_cast<T>(nnbr), rc);
+    return isnan(avg) ? T(0) : avg;
+  }
+
+  // (checks set error bits without leaving the straight-line path; a set
+  // with an error bit is reported, not its values)
   __device__ __forceinline__ T own(specie_id sp, int k) const {
-    const int s = S[sp];
+    const int s = ring_size(sp);
     int lag = k - 1;
     if (lag < 0) lag += s;
     if (static_cast<unsigned>(k) > static_cast<unsigned>(s)) {
@@ -905,10 +918,7 @@ struct WaveContext {
       lag = ((k - 1) % s + s) % s;
     }
     if (lag == 0) return cur[sp];
-    if (lag >= D[sp]) {
-      *err |= kSetUnstagedLag;
-      return T(0);
-    }
+    *err |= lag >= D[sp] ? kSetUnstagedLag : 0;
     return row(sp, lag)[cell];
   }
 
@@ -923,25 +933,21 @@ struct WaveContext {
 #pragma unroll
     for (int e = 0; e < kWaveMaxNbrs; ++e)
       if (e < nnbr) sum += r[nbr[e]];
-    T avg = sum / static_cast<T>(nnbr);
-    return isnan(avg) ? T(0) : avg;
+    return average(sum);
   }
 
   // Lag k mod S.  Lag S-1 is the row DENSE's cell-ordered loop is writing
   // in this step: lower-numbered neighbours (all in lower levels) have
   // their new value there, the others the value of S steps back.
   __device__ __forceinline__ T nbr_avg(specie_id sp, int k) const {
-    const int s = S[sp];
+    const int s = ring_size(sp);
     int lag = k;
     if (static_cast<unsigned>(k) >= static_cast<unsigned>(s)) {
       if (k < 0 || k > s) *err |= kSetBadDelay;
       lag = (k % s + s) % s;
     }
     if (lag == s - 1 && s > 1) {
-      if (D[sp] < s + 1) {
-        *err |= kSetOrderedReads;
-        return T(0);
-      }
+      *err |= D[sp] < s + 1 ? kSetOrderedReads : 0;
       const T* fresh = wrow[sp];
       const T* old = row(sp, lag);
       T sum = T(0);
@@ -950,13 +956,9 @@ struct WaveContext {
         const int v = nbr[e];
         if (e < nnbr) sum += (v < cell ? fresh : old)[v];
       }
-      T avg = sum / static_cast<T>(nnbr);
-      return isnan(avg) ? T(0) : avg;
+      return average(sum);
     }
-    if (lag >= D[sp] - 1) {
-      *err |= kSetUnstagedLag;
-      return T(0);
-    }
+    *err |= lag >= D[sp] - 1 ? kSetUnstagedLag : 0;
     return nbr_lag(sp, lag);
   }
 
@@ -991,8 +993,12 @@ struct WaveContext {
 // shared memory for the whole launch: loaded from the set's history block
 // at entry, stored back at exit.  Records left in global memory are
 // fetched one level ahead.
-template <typename T, bool kKahan, bool kUniform>
-__global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs a, const int* set_list) {
+// kThreads / kMinBlocks: 256 threads, two CTAs per SM (128 registers), or
+// single-warp CTAs with up to 32 per SM (64 registers) for sets whose rows
+// stay in global memory.  kAllShared: every species' rows and the records
+// are in shared memory (the compiler then addresses them as such).
+template <typename T, bool kKahan, bool kUniform, int kThreads, int kMinBlocks, bool kAllShared>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(const StepArgs a, const int* set_list) {
   extern __shared__ __align__(16) unsigned char w_dyn[];
   __shared__ int s_S[kNS], s_D[kNS];
   __shared__ T* s_base[kNS];
@@ -1001,6 +1007,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs 
   __shared__ double s_samples[kMaxAnalyses];
   __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
   __shared__ T* s_rows[kNS];
+  __shared__ T s_rc[kWaveMaxNbrs + 1];  // RN(1 / count)
 
   const int set = set_list[blockIdx.x];
   const SetDesc& sd = a.sets[set];
@@ -1014,6 +1021,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs 
   const int pstride = sd.param_stride;
   const T* P = static_cast<const T*>(a.params) + sd.param_base;
   T* ring = static_cast<T*>(a.ring) + sd.ring_base;
+  for (int i = tid; i <= kWaveMaxNbrs; i += blk) s_rc[i] = i > 0 ? T(1) / static_cast<T>(i) : T(0);
   for (int i = tid; i < kNS; i += blk) {
     s_S[i] = sd.S[i];
     s_D[i] = sd.D[i];
@@ -1034,7 +1042,8 @@ __global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs 
   }
   const uint4* g_rec = a.wave_rec + sd.rec_base;
   const bool rec_shared = sd.topo_off >= 0;
-  const uint4* recs = rec_shared ? reinterpret_cast<const uint4*>(w_dyn + sd.topo_off) : g_rec;
+  const uint4* recs = kAllShared ? reinterpret_cast<const uint4*>(w_dyn + sd.topo_off)
+                                 : (rec_shared ? reinterpret_cast<const uint4*>(w_dyn + sd.topo_off) : g_rec);
   if (rec_shared) {
     uint4* dst = reinterpret_cast<uint4*>(w_dyn + sd.topo_off);
     for (int i = tid; i < n; i += blk) dst[i] = g_rec[i];
@@ -1085,7 +1094,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs 
   for (int sp = 0; sp < kNS; ++sp) {
     lS[sp] = s_S[sp];
     lD[sp] = s_D[sp];
-    lbase[sp] = s_base[sp];
+    lbase[sp] = kAllShared ? reinterpret_cast<T*>(w_dyn + sd.smem_off[sp]) : s_base[sp];
     r0[sp] = static_cast<int>(step % lD[sp]);
   }
 
@@ -1135,7 +1144,8 @@ __global__ void __launch_bounds__(256, 2) dense_step_wave_kernel(const StepArgs 
           for (int sp = 0; sp < kNS; ++sp) cur[sp] = lcur[sp][cell];
           const T* prm = pstride == 0 ? s_prm : P + cell;
           const int ps = pstride == 0 ? 1 : n;
-          WaveContext<T, kUniform> ctx{cur, prm, ps, lS, lD, r0, lbase, lw, nb, cnt, s_olag, s_nlag, n, cell, &err};
+          WaveContext<T, kUniform> ctx{cur,    prm,    ps, lS,   lD,   r0,  lbase, lw, nb, cnt, s_rc[cnt],
+                                       s_olag, s_nlag, n,  cell, &err};
           T dsp[kNS];
 #pragma unroll
           for (int sp = 0; sp < kNS; ++sp) dsp[sp] = T(0);
@@ -1286,6 +1296,15 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
     return cudaGetLastError();                                                                  \
   }
 
+#define DENSE_B200_WAVE_VARIANT(T, KAHAN, UNIFORM, THREADS, MINB, SHARED)                       \
+  {                                                                                             \
+    cudaError_t e = cudaFuncSetAttribute(dense_step_wave_kernel<T, KAHAN, UNIFORM, THREADS, MINB, SHARED>, \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                         kWaveSmemBudget);                                       \
+    if (e != cudaSuccess) return e;                                                             \
+    dense_step_wave_kernel<T, KAHAN, UNIFORM, THREADS, MINB, SHARED><<<n_sets, block, smem, s>>>(a, set_list); \
+  }
+
 #define DENSE_B200_DEFINE_LAUNCHERS(SUFFIX, T, KAHAN)                                             \
   namespace dense_b200 {                                                                        \
   cudaError_t launch_init_##SUFFIX(const StepArgs& a, const double* init_conc,                   \
@@ -1303,19 +1322,17 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
     return cudaGetLastError();                                                                  \
   }                                                                                             \
   cudaError_t launch_step_wave_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets,      \
-                                        int block, int smem, cudaStream_t s) {                  \
+                                        int block, int smem, int all_shared, cudaStream_t s) {  \
     if (n_sets <= 0) return cudaSuccess;                                                        \
-    cudaError_t e;                                                                              \
-    if (a.uniform_params) {                                                                     \
-      e = cudaFuncSetAttribute(dense_step_wave_kernel<T, KAHAN, true>,                          \
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, kWaveSmemBudget);              \
-      if (e != cudaSuccess) return e;                                                           \
-      dense_step_wave_kernel<T, KAHAN, true><<<n_sets, block, smem, s>>>(a, set_list);          \
+    if (all_shared) {                                                                           \
+      if (a.uniform_params) DENSE_B200_WAVE_VARIANT(T, KAHAN, true, 256, 2, true)               \
+      else DENSE_B200_WAVE_VARIANT(T, KAHAN, false, 256, 2, true)                               \
+    } else if (block == 32 && smem <= 2 * 1024) {                                               \
+      if (a.uniform_params) DENSE_B200_WAVE_VARIANT(T, KAHAN, true, 32, 32, false)              \
+      else DENSE_B200_WAVE_VARIANT(T, KAHAN, false, 32, 32, false)                              \
     } else {                                                                                    \
-      e = cudaFuncSetAttribute(dense_step_wave_kernel<T, KAHAN, false>,                         \
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, kWaveSmemBudget);              \
-      if (e != cudaSuccess) return e;                                                           \
-      dense_step_wave_kernel<T, KAHAN, false><<<n_sets, block, smem, s>>>(a, set_list);         \
+      if (a.uniform_params) DENSE_B200_WAVE_VARIANT(T, KAHAN, true, 256, 2, false)              \
+      else DENSE_B200_WAVE_VARIANT(T, KAHAN, false, 256, 2, false)                              \
     }                                                                                           \
     return cudaGetLastError();                                                                  \
   }                                                                                             \

@@ -32,6 +32,7 @@ SCHEDULE_AUTO = 0
 SCHEDULE_MEMORY = 1
 SCHEDULE_GLOBAL = 2
 SCHEDULE_SHARED_NEIGHBOUR = 3
+SCHEDULE_WAVE_GLOBAL = 4
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
@@ -69,6 +70,10 @@ _FUNCS = {
     "dense_engine_plan": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_int64), _I,
                                     _I]),
     "dense_engine_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "dense_graph_capture": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, C.c_int,
+                                      C.POINTER(C.c_void_p)]),
+    "dense_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dense_graph_destroy": (C.c_int, [C.c_void_p]),
     "dense_engine_run_graph": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dense_engine_sync": (C.c_int, [C.c_void_p]),
     "dense_engine_reset": (C.c_int, [C.c_void_p, C.c_void_p]),

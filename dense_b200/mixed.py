@@ -2,11 +2,14 @@
 
 Each model is its own engine library (the model is compiled in, as in
 DENSE), so a mixed batch holds one engine per model.  ``MixedBatch.run``
-replays one CUDA graph that forks every engine's launches onto a stream of
-its own and joins them back, so the models' kernels share the GPU; each
-engine in turn forks its register-kernel and memory-kernel groups.  A step
-of ``num_chunks`` analysis intervals advances every unfinished set.
+replays one CUDA graph (dense_graph_capture) that forks every engine onto a
+branch of its own; each engine in turn forks its kernel groups onto streams
+prioritised by their longest sets, so the models' kernels share the GPU and
+the longest sets start first.  A step of ``num_chunks`` analysis intervals
+advances every unfinished set.
 """
+
+import ctypes as C
 
 import numpy as np
 
@@ -21,38 +24,35 @@ class MixedBatch:
         self.batches = {m: E.Batch(m, sets, step_size, analysis_interval, analyses.get(m, ()), precision, device)
                         for m, sets in groups.items() if sets}
         self._graphs = {}
-        self._streams = None
 
     def _capture(self, num_chunks):
-        import torch
-        if self._streams is None:
-            self._streams = [torch.cuda.Stream(device=self.device) for _ in self.batches]
-            self._main = torch.cuda.Stream(device=self.device)
+        bs = list(self.batches.values())
         # a launch of zero chunks outside capture sets every kernel attribute
-        for b in self.batches.values():
-            b.run(0, stream=self._main.cuda_stream)
-        self._main.synchronize()
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=self._main, capture_error_mode="thread_local"):
-            for st, b in zip(self._streams, self.batches.values()):
-                st.wait_stream(self._main)
-                b.run(num_chunks, stream=st.cuda_stream)
-            for st in self._streams:
-                self._main.wait_stream(st)
+        for b in bs:
+            b.run(0)
+        for b in bs:
+            b.sync()
+        fns = (C.c_void_p * len(bs))(*[C.cast(b.L.lib.dense_engine_run, C.c_void_p).value for b in bs])
+        engs = (C.c_void_p * len(bs))(*[b.h.value for b in bs])
+        g = C.c_void_p()
+        L = bs[0].L
+        L._check(L.lib.dense_graph_capture(len(bs), fns, engs, int(num_chunks), self.device, C.byref(g)))
         return g
 
     def run(self, num_chunks, stream=None):
         """Replay the graph that advances every set by `num_chunks` chunks
-        (captured on first use) on `stream` (a torch stream)."""
-        import torch
+        (captured on first use) on `stream` (a torch stream, or None for the
+        default stream)."""
         g = self._graphs.get(num_chunks)
         if g is None:
             g = self._graphs[num_chunks] = self._capture(num_chunks)
-        if stream is None:
-            g.replay()
-        else:
-            with torch.cuda.stream(stream):
-                g.replay()
+        L = next(iter(self.batches.values())).L
+        L._check(L.lib.dense_graph_launch(g, None if stream is None else C.c_void_p(stream.cuda_stream)))
+
+    def sync(self):
+        """Wait for every launch on the device."""
+        import torch
+        torch.cuda.synchronize(self.device)
 
     def reset(self):
         for b in self.batches.values():
@@ -78,6 +78,10 @@ class MixedBatch:
         return total
 
     def close(self):
+        if self.batches:
+            L = next(iter(self.batches.values())).L
+            for g in self._graphs.values():
+                L.lib.dense_graph_destroy(g)
         self._graphs.clear()
         for b in self.batches.values():
             b.close()

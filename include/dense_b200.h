@@ -68,6 +68,8 @@ extern "C" {
                                               the wave kernel, rows in shared memory as far as they fit */
 #define DENSE_SCHEDULE_GLOBAL 2            /* memory-state kernel with every row in global memory */
 #define DENSE_SCHEDULE_SHARED_NEIGHBOUR 3  /* as MEMORY, but only neighbour-read species in shared memory */
+#define DENSE_SCHEDULE_WAVE_GLOBAL 4       /* as MEMORY, but rows and cell records in global memory: more
+                                              sets per SM (single-warp CTAs up to 32 per SM) */
 
 /* arithmetic of a batch */
 #define DENSE_FP64 0        /* matches DENSE's CPU path bit for bit */
@@ -189,6 +191,17 @@ DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int6
 DENSE_API int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D);
 
 DENSE_API int dense_engine_destroy(dense_engine* e);
+
+/* One CUDA graph over several batches, possibly of different models (no
+   counterpart in DENSE, which runs one model per process): run_fns[i] is
+   the dense_engine_run of engines[i]'s model library; every engine advances
+   num_chunks chunks on a branch of its own, kernels keep their stream
+   priorities.  Run each engine once (e.g. num_chunks 0) before capturing.
+   Launch with dense_graph_launch, free with dense_graph_destroy. */
+DENSE_API int dense_graph_capture(int num_engines, void* const* run_fns, dense_engine* const* engines,
+                                  int num_chunks, int device, void** graph_exec);
+DENSE_API int dense_graph_launch(void* graph_exec, void* stream);
+DENSE_API int dense_graph_destroy(void* graph_exec);
 
 /* Planning without a GPU (no counterpart in DENSE, whose Simulation objects
    size themselves, sim/base.cpp:55-140): per set, the device bytes

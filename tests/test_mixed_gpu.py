@@ -44,7 +44,7 @@ def test_her_every_schedule_bitwise(cells, width, hints):
 
 
 TURING_HINTS = [(0, 0), (1, 32), (1, 64), (E.SCHEDULE_GLOBAL, 0), (E.SCHEDULE_SHARED_NEIGHBOUR, 0),
-                (E.SCHEDULE_GLOBAL, 64)]
+                (E.SCHEDULE_GLOBAL, 64), (E.SCHEDULE_WAVE_GLOBAL, 32), (E.SCHEDULE_WAVE_GLOBAL, 64)]
 
 
 @pytest.mark.parametrize("grid,minutes", [(12, 3.0), (37, 3.0), (64, 0.5)])
@@ -52,7 +52,8 @@ def test_turing_every_schedule_bitwise(grid, minutes):
     """Turing's ordered neighbour reads in the wave kernel (rows in shared
     memory as far as they fit: all species at 12 x 12, the in-order species
     and records at 37 x 37, only the in-order species at 64 x 64), with
-    only neighbour-read species shared, and in the memory kernel with every
+    only neighbour-read species shared, with every row global (single-warp
+    CTAs at 64 registers, or two warps), and in the memory kernel with every
     row global; CTAs of one and two warps."""
     p = workloads.template_params("turing")
     ic = np.array(workloads.templates()["turing"]["init_conc"])
@@ -99,8 +100,8 @@ def test_mixed_graph_matches_plain_runs_and_autotune():
     mb = MixedBatch(tuned, 0.01, 0.1)
     for _ in range(7):  # 7 x 9 chunks cover the 6-minute horizons
         mb.run(9)
+    mb.sync()
     for m, b in mb.batches.items():
-        b.sync()
         assert (b.status() == 0).all()
         for i in range(len(b.sets)):
             assert np.array_equal(b.state(i), plain[m][i], equal_nan=True), (m, i)
