@@ -43,6 +43,9 @@ struct DelayArg {
   __device__ __forceinline__ operator T() const { return prm[(kNR + dr) * pstride]; }
 };
 
+// Neighbour counts whose reciprocals the memory kernel keeps in a table.
+constexpr int kRcTable = 33;
+
 // kUniform: every cell of the set has the set's parameters, so the lag of
 // each (delay reaction, species) read is the same for all cells and is
 // looked up in per-set tables (olag / nlag, [ND][NS]): a value >= 0 is a
@@ -62,6 +65,7 @@ struct DeviceContext {
   int step;                // Euler steps done: lag 0 sits in row step & mask
   const int* nbr;          // this cell's neighbour ids (shared, or global for large lists)
   int nnbr;
+  T rc;                    // RN(1 / nnbr)
   const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
   const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
   bool ordered;            // the set runs in cell-dependency levels (memory kernel)
@@ -95,7 +99,7 @@ struct DeviceContext {
     const T* row = ring + roff[sp] + static_cast<int64_t>((step - lag) & mask[sp]) * n_cells;
     T sum = T(0);
     for (int e = 0; e < nnbr; ++e) sum += row[nbr[e]];
-    T avg = sum / static_cast<T>(nnbr);
+    const T avg = div_by_count(sum, static_cast<T>(nnbr), rc);
     return isnan(avg) ? T(0) : avg;
   }
 
@@ -123,7 +127,7 @@ struct DeviceContext {
         const int v = nbr[e];
         sum += v < cell ? fresh[v] : old[v];
       }
-      T avg = sum / static_cast<T>(nnbr);
+      const T avg = div_by_count(sum, static_cast<T>(nnbr), rc);
       return isnan(avg) ? T(0) : avg;
     }
     if (lag >= m) {
@@ -580,7 +584,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   T* ring = static_cast<T*>(a.ring) + sd.ring_base;
   int64_t step = pg.step;
   DeviceContext<T, kUniform> ctx{cur,  prm,    ps,   s_kd + cell, blk,    s_S,    s_mask, s_roff, ring,
-                                 static_cast<int>(step), nbr, nnbr, s_olag, s_nlag, false, n, cell, &err};
+                                 static_cast<int>(step), nbr, nnbr, T(1) / static_cast<T>(nnbr), s_olag, s_nlag,
+                                 false, n, cell, &err};
 
   const T dt = static_cast<T>(a.dt);
   int chunk = pg.chunk;
@@ -725,6 +730,7 @@ __device__ __forceinline__ void fill_lag_tables(const T* s_prm, const int* s_S, 
 // one level holding every cell.
 template <typename T, bool kKahan, bool kUniform>
 __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a, const int* set_list) {
+  __shared__ T s_rc[kRcTable];  // RN(1 / count) for neighbour counts below kRcTable
   __shared__ int s_S[kNS], s_mask[kNS];
   __shared__ int64_t s_roff[kNS];
   __shared__ T s_prm[kNP];
@@ -744,6 +750,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
 
   const int pstride = sd.param_stride;
   const T* P = static_cast<const T*>(a.params) + sd.param_base;
+  for (int i = tid; i < kRcTable; i += blk) s_rc[i] = i > 0 ? T(1) / static_cast<T>(i) : T(0);
   for (int i = tid; i < kNS; i += blk) {  // blocks may be a single warp
     s_S[i] = sd.S[i];
     s_mask[i] = sd.D[i] - 1;
@@ -803,8 +810,10 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
           const T* prm = pstride == 0 ? s_prm : P + cell;
           const int ps = pstride == 0 ? 1 : n;
           const int nb0 = nbr_off[cell];
+          const int cnt = nbr_off[cell + 1] - nb0;
           DeviceContext<T, kUniform> ctx{cur,    prm,    ps,     nullptr, 0,      s_S,  s_mask, s_roff,
-                                         ring,   st32,   a.nbr_idx + nb0, nbr_off[cell + 1] - nb0,
+                                         ring,   st32,   a.nbr_idx + nb0, cnt,
+                                         cnt < kRcTable ? s_rc[cnt] : T(1) / static_cast<T>(cnt),
                                          s_olag, s_nlag, ordered, n,      cell,   &err};
           T dsp[kNS];
 #pragma unroll
