@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <limits>
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -76,6 +77,8 @@ struct LagTracer {
   bool* ordered;  // a neighbour read of lag S-1
   bool* bad;
   bool* ord_sp;   // [NS] species read by neighbours at lag S-1
+  int* plain_min; // [NS] shallowest other neighbour lag (INT_MAX none)
+  int* plain_max; // [NS] deepest other neighbour lag (-1 none)
   double getCon(specie_id sp) const { return conc[sp]; }
   double getCon(specie_id sp, int k) const {
     const int s = S[sp];
@@ -88,7 +91,12 @@ struct LagTracer {
     const int s = S[sp];
     if (k < 0 || k > s) *bad = true;
     const int lag = ((k % s) + s) % s;
-    if (lag == s - 1 && s > 1) *ordered = ord_sp[sp] = true;
+    if (lag == s - 1 && s > 1) {
+      *ordered = ord_sp[sp] = true;
+    } else {
+      plain_min[sp] = std::min(plain_min[sp], lag);
+      plain_max[sp] = std::max(plain_max[sp], lag);
+    }
     nbr_max[sp] = std::max(nbr_max[sp], lag);
     return nbr_value;
   }
@@ -340,6 +348,11 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
   for (int sp = 0; sp < NUM_SPECIES; ++sp) { own_max[sp] = 0; nbr_max[sp] = -1; }
   bool ordered = false, bad = false;
   bool ord_sp[NUM_SPECIES] = {};
+  int plain_min[NUM_SPECIES], plain_max[NUM_SPECIES];
+  for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+    plain_min[sp] = std::numeric_limits<int>::max();
+    plain_max[sp] = -1;
+  }
   double prm[NUM_PARAMS];
   double conc[NUM_SPECIES];
   const double nbr_values[4] = {0.0, 2.0, 0.5, 7.25};
@@ -349,7 +362,7 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
     for (int i = 0; i < NUM_PARAMS; ++i) prm[i] = cell_params[static_cast<size_t>(i) * pcols + c];
     for (int pass = 0; pass < 4; ++pass) {
       for (int sp = 0; sp < NUM_SPECIES; ++sp) conc[sp] = pass == 0 ? 0.0 : (pass == 1 ? 1.0 : 0.37 * (sp + pass));
-      LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad, ord_sp};
+      LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad, ord_sp, plain_min, plain_max};
 #define REACTION(name) reaction<name>::active_rate(t);
 #include "reactions_list.hpp"
 #undef REACTION
@@ -418,6 +431,59 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
     }
     d.lvl_smem_off = static_cast<int>(used);
     d.smem_bytes = static_cast<int>(used + lvl_bytes);
+  }
+  // Time pipelining of the wave kernel.  Step k's level l runs in interval
+  // T(k, l) = k * delta + l, intervals separated by barriers.  A read of a
+  // neighbour v's row must come after the interval that wrote it and
+  // before the one that overwrites its slot (rows are kept modulo D):
+  //   lag-(S-1) read of v > c: row k+1-S, written in step k-S and rewritten
+  //     in step k-S+D:   l_v - l_c < S delta,   l_c - l_v < (D - S) delta;
+  //   read at another lag m:  l_v - l_c < (m + 1) delta,
+  //                           l_c - l_v < (D - m - 1) delta;
+  //   lag-(S-1) read of v < c reads this step's row (lower levels) only.
+  // delta is the least integer meeting every such bound; the steps in flight
+  // are ceil(L / delta), at most kWaveMaxFronts.
+  d.wave_delta = 0;
+  d.wave_fronts = 1;
+  if (plan.wave) {
+    const int L = static_cast<int>(plan.lvl_off.size()) - 1;
+    std::vector<int> level(n, 0);
+    for (int l = 0; l < L; ++l)
+      for (int i = plan.lvl_off[l]; i < plan.lvl_off[l + 1]; ++i) level[plan.lvl_cells[i]] = l;
+    int64_t delta = 1;
+    bool pipe = true;
+    // delta > num / den
+    auto need = [&](int64_t num, int64_t den) {
+      if (den <= 0) {
+        if (num >= 0) pipe = false;
+        return;
+      }
+      if (num >= 0) delta = std::max(delta, num / den + 1);
+    };
+    for (int c = 0; c < n && pipe; ++c)
+      for (int k = in.nbr_offsets[c]; k < in.nbr_offsets[c + 1]; ++k) {
+        const int v = in.nbr_ids[k];
+        const int64_t dl = level[v] - level[c];
+        for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+          if (ord_sp[sp] && v > c) {
+            need(dl, d.S[sp]);
+            need(-dl, d.D[sp] - d.S[sp]);
+          }
+          if (plain_max[sp] >= 0) {
+            need(dl, plain_min[sp] + 1);
+            need(-dl, d.D[sp] - plain_max[sp] - 1);
+          }
+        }
+      }
+    int fronts = pipe ? static_cast<int>((L + delta - 1) / delta) : 1;
+    fronts = std::max(1, std::min(fronts, kWaveMaxFronts));
+    // fewer fronts than the bound allows: space the steps further apart
+    delta = std::max<int64_t>(delta, (L + fronts - 1) / fronts);
+    d.wave_delta = static_cast<int>(std::max<int64_t>(delta, 1));
+    d.wave_fronts = fronts;
+    // a thread group per front, the whole CTA at most 256 threads
+    const int group = std::max(32, std::min(plan.mem_block, 256 / fronts / 32 * 32));
+    plan.mem_block = group * fronts;
   }
   // chunk count: a = 0, 1, ... while a < duration / interval
   return DENSE_OK;
@@ -631,7 +697,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       double m = 0;
       for (int j = g[3]; j < g[3] + g[4]; ++j) {
         const SetDesc& d = e->sets[mem_list[j]];
-        const double per_step = g[0] ? d.n_levels : d.n_levels * std::ceil(static_cast<double>(d.n_cells) /
+        const double per_step = g[0] ? d.wave_delta : d.n_levels * std::ceil(static_cast<double>(d.n_cells) /
                                                                             (d.n_levels * g[1]));
         m = std::max(m, static_cast<double>(d.n_chunks) * d.steps_per_chunk * per_step);
       }

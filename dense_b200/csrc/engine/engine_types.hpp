@@ -89,6 +89,10 @@ struct SetDesc {
   int topo_off;          // byte offset of the records in shared memory, -1: global
   int smem_bytes;        // dynamic shared memory the set needs
   int64_t rec_base;      // first record of the set in StepArgs::wave_rec
+  // time pipelining: step k + 1 runs wave_delta levels behind step k, so
+  // wave_fronts consecutive steps are in flight, one thread group each
+  int wave_delta;
+  int wave_fronts;
 };
 
 // Dynamic shared memory a wave-kernel CTA may use (the 227 KB opt-in limit
@@ -96,6 +100,7 @@ struct SetDesc {
 // neighbours a wave-kernel cell record holds.
 constexpr int kWaveSmemBudget = 227 * 1024 - 8 * 1024;
 constexpr int kWaveMaxNbrs = 6;
+constexpr int kWaveMaxFronts = 4;   // steps in flight in the wave kernel
 
 // Mutable per-set progress, updated by the kernels.
 struct SetProgress {

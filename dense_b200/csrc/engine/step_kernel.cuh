@@ -1104,8 +1104,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
     lS[sp] = s_S[sp];
     lD[sp] = s_D[sp];
     lbase[sp] = kAllShared ? reinterpret_cast<T*>(w_dyn + sd.smem_off[sp]) : s_base[sp];
-    r0[sp] = static_cast<int>(step % lD[sp]);
+    r0[sp] = 0;
+    lcur[sp] = lw[sp] = lbase[sp];
   }
+  // thread groups, one per wavefront
+  const int fronts = sd.wave_fronts;
+  const int delta = sd.wave_delta;
+  const int gsz = blk / fronts;
+  const int grp = tid / gsz, gtid = tid % gsz;
 
   for (; chunk < chunk_end; ++chunk) {
     if (a.n_analyses > 0) {
@@ -1123,26 +1129,32 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
         break;
       }
     }
-    for (int s = 0; s < sd.steps_per_chunk; ++s) {
-      int rw[kNS];  // row this step writes
+    // the chunk's steps as overlapping wavefronts: in interval tau, group g
+    // runs level tau - k * delta of the one step k in flight with
+    // k = g (mod fronts); a barrier closes each interval
+    const int S_chunk = sd.steps_per_chunk;
+    const int n_intervals = S_chunk > 0 ? (S_chunk - 1) * delta + n_levels : 0;
+    int kcur = -1;
+    int rw[kNS];
+    for (int tau = 0; tau < n_intervals; ++tau) {
+      int kk = tau / delta;
+      kk -= ((kk - grp) % fronts + fronts) % fronts;
+      const int l = tau - kk * delta;
+      if (grp < fronts && kk >= 0 && kk < S_chunk && l < n_levels) {
+        if (kk != kcur) {
+          // rows of step `step + kk`
+          kcur = kk;
 #pragma unroll
-      for (int sp = 0; sp < kNS; ++sp) {
-        rw[sp] = r0[sp] + 1 == lD[sp] ? 0 : r0[sp] + 1;
-        lcur[sp] = lbase[sp] + r0[sp] * n;
-        lw[sp] = lbase[sp] + rw[sp] * n;
-      }
-      uint4 pre = make_uint4(0, 0, 0, 0);
-      if (!rec_shared && tid < t_lvl[1]) pre = recs[tid];
-      for (int l = 0; l < n_levels; ++l) {
-        const int i0 = t_lvl[l], i1 = t_lvl[l + 1];
-        uint4 here = pre;
-        if (!rec_shared && l + 1 < n_levels) {
-          // the next level's first record of this thread, fetched now
-          const int inext = i1 + tid;
-          if (inext < t_lvl[l + 2]) pre = recs[inext];
+          for (int sp = 0; sp < kNS; ++sp) {
+            r0[sp] = static_cast<int>((step + kk) % lD[sp]);
+            rw[sp] = r0[sp] + 1 == lD[sp] ? 0 : r0[sp] + 1;
+            lcur[sp] = lbase[sp] + r0[sp] * n;
+            lw[sp] = lbase[sp] + rw[sp] * n;
+          }
         }
-        for (int i = i0 + tid; i < i1; i += blk) {
-          const uint4 raw = (rec_shared || i != i0 + tid) ? recs[i] : here;
+        const int i1 = t_lvl[l + 1];
+        for (int i = t_lvl[l] + gtid; i < i1; i += gsz) {
+          const uint4 raw = recs[i];
           const int cell = static_cast<int>(raw.x & 0xFFFFu);
           const int cnt = static_cast<int>(raw.x >> 16);
           const uint16_t nb[6] = {static_cast<uint16_t>(raw.y & 0xFFFFu), static_cast<uint16_t>(raw.y >> 16),
@@ -1181,12 +1193,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
             lw[sp][cell] = nxt;
           }
         }
-        __syncthreads();
       }
-#pragma unroll
-      for (int sp = 0; sp < kNS; ++sp) r0[sp] = rw[sp];
-      ++step;
+      __syncthreads();
     }
+    step += S_chunk;
     age += a.interval;
   }
 

@@ -79,8 +79,9 @@ def test_report_number_format():
 
 def test_plan_kernels_and_bytes():
     """dense_engine_plan (no GPU): register kernel for unordered sets of at
-    most 256 cells, memory kernel above that or on request, a CTA the width
-    of the widest dependency level for ordered (Turing) sets, hints checked."""
+    most 256 cells, memory kernel above that or on request, for ordered
+    (Turing) sets a thread group the width of the widest dependency level
+    per step in flight, hints checked."""
     from dense_b200 import tissue, workloads
     from dense_b200.engine import DenseError, ParameterSet, SCHEDULE_MEMORY, plan
     p = workloads.template_params()
@@ -100,7 +101,8 @@ def test_plan_kernels_and_bytes():
         off, ids = tissue.default_graph(N * N, N)
         ts.append(ParameterSet(off, ids, tp, duration=10))
     _, kernel, levels = plan("turing", ts, 0.01, 1.0)
-    assert list(kernel) == [32, 32, 32] and (levels > 1).all()
+    # wave kernel: one warp per level, three steps in flight
+    assert list(kernel) == [96, 96, 96] and (levels > 1).all()
     with pytest.raises(DenseError):
         plan("her_model_2014", [ParameterSet(off, ids, tp, duration=10)], 0.01, 1.0)
     off, ids = tissue.default_graph(200, 4)

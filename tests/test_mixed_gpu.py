@@ -96,7 +96,7 @@ def test_mixed_graph_matches_plain_runs_and_autotune():
     tuner = Autotuner(sample_sets=2, minutes=0.2)
     for m, sets in tuned.items():
         chosen = tuner.tune(m, sets, 0.01)
-        assert chosen and all(s.schedule in (0, 1, 2, 3) for s in sets)
+        assert chosen and all(s.schedule in (0, 1, 2, 3, 4) for s in sets)
     mb = MixedBatch(tuned, 0.01, 0.1)
     for _ in range(7):  # 7 x 9 chunks cover the 6-minute horizons
         mb.run(9)
