@@ -4,7 +4,9 @@ A set's results do not depend on how it is scheduled, only its speed does:
 the register kernel (one thread per cell, the whole state in registers;
 unordered sets of at most 256 cells) or the memory-state kernel with a CTA
 of 32..256 threads (any set; cells beyond the CTA width loop, so the CTA
-size is the cells-per-thread knob).  History depth is not a knob: each
+size is the cells-per-thread knob), or for sets with in-order neighbour
+reads the wave kernel, whose CTA holds one thread group per time step in
+flight (so there the CTA size also sets how many steps overlap).  History depth is not a knob: each
 species' ring holds exactly the lags its reads need, rounded up to a power
 of two.
 
@@ -49,9 +51,11 @@ def candidates(ordered, cells_log2, default_block):
         if b <= limit:
             out.append((E.SCHEDULE_MEMORY, b))
     if ordered:
-        out.append((E.SCHEDULE_SHARED_NEIGHBOUR, default_block))
-        # every row global: more sets per SM, longer levels
-        out.append((E.SCHEDULE_WAVE_GLOBAL, default_block))
+        # the wave kernel's CTA is one thread group per step in flight: the
+        # engine's choice, or one or two warps (fewer steps in flight, more
+        # sets per SM)
+        out = [(E.SCHEDULE_MEMORY, 0), (E.SCHEDULE_MEMORY, 32), (E.SCHEDULE_MEMORY, 64),
+               (E.SCHEDULE_SHARED_NEIGHBOUR, 0), (E.SCHEDULE_WAVE_GLOBAL, 0)]
     return out
 
 

@@ -477,12 +477,18 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
       }
     int fronts = pipe ? static_cast<int>((L + delta - 1) / delta) : 1;
     fronts = std::max(1, std::min(fronts, kWaveMaxFronts));
+    // a CTA-size hint caps the fronts at one warp each
+    if (in.mem_block > 0) fronts = std::max(1, std::min(fronts, in.mem_block / 32));
     // fewer fronts than the bound allows: space the steps further apart
     delta = std::max<int64_t>(delta, (L + fronts - 1) / fronts);
     d.wave_delta = static_cast<int>(std::max<int64_t>(delta, 1));
     d.wave_fronts = fronts;
-    // a thread group per front, the whole CTA at most 256 threads
-    const int group = std::max(32, std::min(plan.mem_block, 256 / fronts / 32 * 32));
+    // a thread group per front: the widest level in warps, or the hint's
+    // share; the whole CTA at most 256 threads
+    int widest = 0;
+    for (int l = 0; l < L; ++l) widest = std::max(widest, plan.lvl_off[l + 1] - plan.lvl_off[l]);
+    int group = in.mem_block > 0 ? in.mem_block / fronts : (widest + 31) / 32 * 32;
+    group = std::max(32, std::min(group, 256 / fronts) / 32 * 32);
     plan.mem_block = group * fronts;
   }
   // chunk count: a = 0, 1, ... while a < duration / interval
