@@ -120,7 +120,9 @@ int grid_for(int64_t n) {
 // for the shape rules.  err (device int) collects kErr* bits.
 MLP_API int dense_mlp_gemm(const void* A, int lda, const void* B, int ldb, float* D, int ldd, int M, int N, int K,
                            int epilogue, const float* bias, void* H, int ldh, int* err, void* stream) {
-  if ((M % kTileM) || (N % 16) || N < 16 || N > 256 || (K % kChunkK) || (lda % 8) || (ldb % 8)) return 1;
+  if ((M % kTileM) || (N % 16) || N < 16 || N > 256 || (K % kChunkK) || (lda % 8) || (ldb % 8) || (ldd % 4) ||
+      (epilogue == kEpiBiasGelu && (ldh % 8)))
+    return 1;
   const size_t smem = umma_gemm_smem(N);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const auto* a = static_cast<const __nv_bfloat16*>(A);

@@ -4,17 +4,18 @@
 //   D[M][N] (FP32) = A[M][K] (BF16, row-major) . B[N][K]^T (BF16, row-major)
 //
 // with M a multiple of 128, N a multiple of 16 in [16, 256], K a multiple
-// of 64, and 16-byte aligned rows.  One CTA of 128 threads computes a
-// 128 x N tile: the accumulator lives in tensor memory (N columns, one TMEM
-// lane per output row), A and B stream through shared memory in chunks of
-// 64 along K in the no-swizzle K-major layout the UMMA descriptors expect
-// (8-row x 16-byte core matrices; the two core matrices of one K=16 step
-// 128 bytes apart, 8-row groups 1024 bytes apart).  One elected thread
-// issues four tcgen05.mma (M=128, N, K=16) per chunk and commits them to an
-// mbarrier; every thread waits on it (with an iteration limit) before the
-// chunk buffer is refilled.  The epilogue reads the accumulator with
-// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31) and applies the layer's
-// bias and activation.
+// of 64, and 16-byte aligned rows (lda, ldb, ldh multiples of 8, ldd of 4).
+// One CTA of 128 threads computes a 128 x N tile: the accumulator lives in
+// tensor memory (N columns, one TMEM lane per output row), A and B stream
+// through shared memory in chunks of 64 along K in the no-swizzle K-major
+// layout the UMMA descriptors expect (8-row x 16-byte core matrices; the
+// two core matrices of one K=16 step 128 bytes apart, 8-row groups 1024
+// bytes apart).  One elected thread issues four tcgen05.mma (M=128, N,
+// K=16) per chunk and commits them to an mbarrier; every thread waits on it
+// (with an iteration limit) before the chunk buffer is refilled.  The
+// epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31), adds the layer's bias and activation and writes 16-byte
+// vectors.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_flag;
+  __shared__ float s_bias[256];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int row0 = blockIdx.x * kTileM;
@@ -116,6 +118,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
     abort_flag = 0;
   }
+  if (EPI != kEpiStore)
+    for (int i = tid; i < N; i += kGemmThreads) s_bias[i] = bias[i];
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -170,6 +174,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
   if (!abort_flag) {
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = output rows
+    // warp w reads TMEM lanes 32w..32w+31, the accumulator rows of its threads
     const int row = row0 + warp * 32 + lane;
     for (int c0 = 0; c0 < N; c0 += 16) {
       uint32_t r[16];
@@ -181,13 +186,24 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      // 16 consecutive columns of this thread's row: four 16-byte stores
+      // (and two for the BF16 activations)
+      float v[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        float v = __uint_as_float(r[j]);
-        const int col = c0 + j;
-        if (EPI != kEpiStore) v += bias[col];
-        D[static_cast<size_t>(row) * ldd + col] = v;
-        if (EPI == kEpiBiasGelu) H[static_cast<size_t>(row) * ldh + col] = __float2bfloat16(gelu(v));
+      for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]) + (EPI != kEpiStore ? s_bias[c0 + j] : 0.f);
+      float4* drow = reinterpret_cast<float4*>(D + static_cast<size_t>(row) * ldd + c0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) drow[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+      if (EPI == kEpiBiasGelu) {
+        uint32_t hp[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(v[2 * j]), gelu(v[2 * j + 1]));
+          hp[j] = *reinterpret_cast<const uint32_t*>(&h2);
+        }
+        uint4* hrow = reinterpret_cast<uint4*>(H + static_cast<size_t>(row) * ldh + c0);
+        hrow[0] = make_uint4(hp[0], hp[1], hp[2], hp[3]);
+        hrow[1] = make_uint4(hp[4], hp[5], hp[6], hp[7]);
       }
     }
   }
