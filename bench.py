@@ -287,6 +287,60 @@ def run_mixed(a):
         torch.distributed.destroy_process_group()
 
 
+def run_turing(a):
+    """Turing-Pattern sets of one N x N grid (`--grid`), template parameters,
+    the model's initial concentrations, dt 0.01 min, no analyses: the wave
+    kernel alone."""
+    import torch
+    import numpy as np
+    from dense_b200 import engine as E, workloads
+    from dense_b200.tissue import default_graph
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    N = a.grid
+    sets_n = a.sets if a.sets != 4096 else 148 * 6
+    p = workloads.template_params("turing")
+    ic = np.array(workloads.templates()["turing"]["init_conc"])
+    off, ids = default_graph(N * N, N)
+    sets = [E.ParameterSet(off, ids, p, init_conc=ic, duration=a.minutes) for _ in range(sets_n)]
+    b = E.Batch("turing", sets, 0.01, 1.0 if a.minutes >= 1.0 else a.minutes, (), device=local)
+    total_chunks = int(math.ceil(a.minutes / (1.0 if a.minutes >= 1.0 else a.minutes)))
+    per_step = int(math.ceil(total_chunks / a.steps))
+    stream = torch.cuda.Stream()
+    for _ in range(a.warmup):
+        b.run(per_step, stream=stream.cuda_stream, graph=True)
+    b.reset(stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    clocks = Clocks(local)
+    ev[0].record(stream)
+    for k in range(a.steps):
+        b.run(per_step, stream=stream.cuda_stream, graph=True)
+        ev[k + 1].record(stream)
+    stream.synchronize()
+    clk = clocks.stop()
+    ms = ev[0].elapsed_time(ev[a.steps])
+    chunks, _ = b.progress()
+    spc = b.info()["total_cell_steps"] // max(1, total_chunks) // sets_n // (N * N)
+    done = int(chunks.astype(np.int64).sum()) * spc * N * N
+    value = done / (ms / 1e3)
+    hbm, peak_src = peaks()
+    achieved = TURING_BYTES_PER_CELL_STEP * value / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "Turing-Pattern %d sets of a %dx%d grid (-c %d -w %d), template parameters, "
+                                   "dt 0.01 min, %g min, no analyses" % (sets_n, N, N, N * N, N, a.minutes)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "basis": "%d algorithmic bytes per Turing cell-step; peak %s"
+                                                   % (TURING_BYTES_PER_CELL_STEP, peak_src)},
+            "gpu_launches": a.steps, "clocks": clk,
+            "status_nonzero_sets": int((b.status() != 0).sum())}), flush=True)
+    b.close()
+
+
 def _ref_worker(args):
     seed, minutes = args
     r = cpu_sample("reference", num_sets=1, minutes=minutes, seed=seed)
@@ -339,14 +393,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--analyses", default="oscillation", choices=["oscillation", "none"],
                     help="the workload's analyses: Oscillation(mh1) every 0.1 min, or none")
-    ap.add_argument("--workload", default="batch", choices=["batch", "mixed"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "mixed", "turing"],
                     help="batch: 4096 her_model_2014 sets of 200 cells; mixed: the uneven her + Turing batch "
-                         "(10000 sets unless --sets is given)")
+                         "(10000 sets unless --sets is given); turing: sets of one Turing grid (--grid)")
+    ap.add_argument("--grid", type=int, default=64, help="turing workload: grid side N")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "mixed":
         return run_mixed(a)
+    if a.workload == "turing":
+        return run_turing(a)
 
     import torch
     rank, world, local = dist_env()

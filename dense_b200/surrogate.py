@@ -284,3 +284,47 @@ class MLP:
 
     def state(self):
         return {"W": [w.cpu().numpy() for w in self.W], "b": [b.cpu().numpy() for b in self.b]}
+
+
+def bench_gemm(rows=131072, reps=20, device=0):
+    """Times the tensor-core GEMM on the MLP's layer shapes (BF16 inputs,
+    FP32 outputs): rows x 256 x 64 (first layer), rows x 256 x 256 (hidden
+    layers), rows x 128 x 256 (output layer), plain and with the bias+GELU
+    epilogue; one dict per shape and epilogue, CUDA-event timed."""
+    import torch
+    k = Kernels(device)
+    dev = "cuda:%d" % device
+    out = []
+    for (n, kk) in ((256, 64), (256, 256), (128, 256)):
+        A = torch.randn(rows, kk, device=dev).to(torch.bfloat16)
+        B = torch.randn(n, kk, device=dev).to(torch.bfloat16)
+        D = torch.empty(rows, n, device=dev, dtype=torch.float32)
+        H = torch.empty(rows, n, device=dev, dtype=torch.bfloat16)
+        bias = torch.randn(n, device=dev)
+        for epi, name in ((EPI_STORE, "store"), (EPI_BIAS_GELU, "bias_gelu")):
+            k.gemm(A, B, D, epi, bias, H)
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s = torch.cuda.current_stream(device)
+            e0.record(s)
+            for _ in range(reps):
+                k.gemm(A, B, D, epi, bias, H)
+            e1.record(s)
+            torch.cuda.synchronize(device)
+            ms = e0.elapsed_time(e1) / reps
+            nbytes = rows * kk * 2 + n * kk * 2 + rows * n * 4 + (rows * n * 2 if epi == EPI_BIAS_GELU else 0)
+            out.append({"rows": rows, "n": n, "k": kk, "epilogue": name, "us": ms * 1e3,
+                        "tflops": 2.0 * rows * n * kk / ms / 1e9, "gbs": nbytes / ms / 1e6})
+    k.check()
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="time the surrogate's tensor-core GEMM")
+    ap.add_argument("--rows", type=int, default=131072)
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    for r in bench_gemm(a.rows, a.reps):
+        print(json.dumps(r))
