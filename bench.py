@@ -47,6 +47,7 @@ sys.path.insert(0, ROOT)
 #         delta terms (mul + add) and 14 Euler updates (mul + add) = 221.
 BYTES_PER_CELL_STEP = 304
 FLOPS_PER_CELL_STEP = 221
+DRAM_BYTES_PER_CELL_STEP = 17.7
 
 METRIC = "cell-steps/s (FP64 plain)"
 
@@ -488,14 +489,13 @@ def main():
 
     hbm, peak_src = peaks()
     achieved_gbs = BYTES_PER_CELL_STEP * per_launch_cell_steps / avg_launch_s / 1e9
+    # DRAM traffic of one launch, scaled from an ncu capture of a smaller
+    # launch of the same kernel and workload shape (296 sets x 200 cells x
+    # 1000 steps: dram__bytes_read.sum + dram__bytes_write.sum = 1.048 GB,
+    # 17.7 B per cell-step, cold caches); FP64 with Oscillation only
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            d = json.load(f)
-        traffic = d.get("bytes_per_cell_step", None)
-        if traffic is not None:
-            traffic = traffic * per_launch_cell_steps
+    if precision == E.FP64 and analyses:
+        traffic = DRAM_BYTES_PER_CELL_STEP * per_launch_cell_steps
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
