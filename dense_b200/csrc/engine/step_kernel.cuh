@@ -583,8 +583,24 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   int err = 0;
   T* ring = static_cast<T*>(a.ring) + sd.ring_base;
   int64_t step = pg.step;
-  DeviceContext<T, kUniform> ctx{cur,  prm,    ps,   s_kd + cell, blk,    s_S,    s_mask, s_roff, ring,
-                                 static_cast<int>(step), nbr, nnbr, T(1) / static_cast<T>(nnbr), s_olag, s_nlag,
+  // per-set constants of the history reads in registers (only the entries
+  // the model's reads use stay live); through shared memory they would be
+  // reloaded after every ring store
+  int64_t lroff[kNS];
+  int lmask[kNS];
+#pragma unroll
+  for (int sp = 0; sp < kNS; ++sp) {
+    lroff[sp] = s_roff[sp];
+    lmask[sp] = s_mask[sp];
+  }
+  int lolag[kND > 0 ? kND * kNS : 1], lnlag[kND > 0 ? kND * kNS : 1];
+#pragma unroll
+  for (int i = 0; i < kND * kNS; ++i) {
+    lolag[i] = s_olag[i];
+    lnlag[i] = s_nlag[i];
+  }
+  DeviceContext<T, kUniform> ctx{cur,  prm,    ps,   s_kd + cell, blk,    s_S,    lmask, lroff, ring,
+                                 static_cast<int>(step), nbr, nnbr, T(1) / static_cast<T>(nnbr), lolag, lnlag,
                                  false, n, cell, &err};
 
   const T dt = static_cast<T>(a.dt);
