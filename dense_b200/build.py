@@ -109,9 +109,27 @@ def build_cli(model, force=False):
     return out
 
 
+def csv_gen_path(model):
+    return os.path.join(LIB_DIR, "dense_csv_gen_%s" % model)
+
+
+def build_csv_gen(model, force=False):
+    """DENSE's `csv_gen` for the model (csrc/cli/csv_gen_main.cpp): the
+    parameter-file templates, from the engine library's model tables."""
+    lib = build_model(model, force)
+    out = csv_gen_path(model)
+    src = os.path.join(CSRC, "cli", "csv_gen_main.cpp")
+    if not force and _up_to_date(out, [src, lib, os.path.join(INCLUDE, "dense_b200.h")]):
+        return out
+    _run(["g++", "-O2", "-std=c++17", "-I", INCLUDE, src, "-o", out, "-L", LIB_DIR,
+          "-l:" + os.path.basename(lib), "-Wl,-rpath,$ORIGIN"])
+    return out
+
+
 def build_all(models=None, force=False):
     out = {}
     for m in (models or MODEL_DIRS):
         out[m] = build_model(m, force)
         build_cli(m, force)
+        build_csv_gen(m, force)
     return out

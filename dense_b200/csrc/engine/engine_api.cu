@@ -526,6 +526,12 @@ int dense_model_get_info(dense_model_info* out) {
 
 const char* dense_model_specie_name(int i) { return (i >= 0 && i < NUM_SPECIES) ? dense_specie_names[i] : nullptr; }
 const char* dense_model_reaction_name(int i) { return (i >= 0 && i < NUM_REACTIONS) ? dense_reaction_names[i] : nullptr; }
+const char* dense_model_delay_reaction_name(int d) {
+  return (d >= 0 && d < NUM_DELAY_REACTIONS) ? dense_reaction_names[dense_delay_reaction_of[d]] : nullptr;
+}
+const char* dense_model_critical_specie_name(int c) {
+  return (c >= 0 && c < NUM_CRITICAL_SPECIES) ? dense_specie_names[dense_critical_species_of[c]] : nullptr;
+}
 const char* dense_last_error(void) { return g_error.c_str(); }
 
 int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set_desc* in_sets,

@@ -65,6 +65,8 @@ _FUNCS = {
     "dense_model_get_info": (C.c_int, [C.POINTER(_ModelInfo)]),
     "dense_model_specie_name": (C.c_char_p, [C.c_int]),
     "dense_model_reaction_name": (C.c_char_p, [C.c_int]),
+    "dense_model_delay_reaction_name": (C.c_char_p, [C.c_int]),
+    "dense_model_critical_specie_name": (C.c_char_p, [C.c_int]),
     "dense_last_error": (C.c_char_p, []),
     "dense_engine_create": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_void_p)]),
     "dense_engine_plan": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_int64), _I,
@@ -115,6 +117,10 @@ class ModelLibrary:
         self.num_params = info.num_params
         self.species = [self.lib.dense_model_specie_name(i).decode() for i in range(self.num_species)]
         self.reactions = [self.lib.dense_model_reaction_name(i).decode() for i in range(self.num_reactions)]
+        self.delay_reactions = [self.lib.dense_model_delay_reaction_name(i).decode()
+                                for i in range(self.num_delay_reactions)]
+        self.critical_species = [self.lib.dense_model_critical_specie_name(i).decode()
+                                 for i in range(self.num_critical_species)]
 
     def _check(self, rc):
         if rc != 0:

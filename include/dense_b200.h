@@ -132,6 +132,11 @@ typedef struct dense_engine dense_engine;
 DENSE_API int dense_model_get_info(dense_model_info* out);
 DENSE_API const char* dense_model_specie_name(int species);
 DENSE_API const char* dense_model_reaction_name(int reaction);
+/* Reaction name of delay reaction d (reactions_list.hpp order of the
+   DELAY_REACTION entries), and species name of critical species c
+   (specie_list.hpp order of the CRITICAL_SPECIE entries); NULL out of range. */
+DENSE_API const char* dense_model_delay_reaction_name(int d);
+DENSE_API const char* dense_model_critical_specie_name(int c);
 DENSE_API const char* dense_last_error(void);
 
 /* Validate and stage a batch on the device (host buffers are copied). */

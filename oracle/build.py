@@ -12,7 +12,8 @@ Three kinds of artefact, per DENSE model:
   with ref_harness.cpp, which drives them through the oracle's C interface.
 * ``oracle/_ref/<model>_simulation`` -- DENSE's own ``simulation`` CLI for
   the model (deterministic_main.cpp), for byte-level checks of its CSV
-  output.
+  output; ``oracle/_ref/<model>_csv_gen`` -- DENSE's ``csv_gen`` (the
+  parameter-file templates), for the same check of ours.
 
 The DENSE tree is ``$DENSE_REF_DIR`` (default /root/reference).  When it
 is absent (a machine that only runs the prebuilt libraries) the reference
@@ -87,6 +88,14 @@ def ref_cli_path(model):
     return os.path.join(REF_DIR, "%s_simulation" % model)
 
 
+def ref_csv_gen_path(model):
+    return os.path.join(REF_DIR, "%s_csv_gen" % model)
+
+
+REF_CSV_GEN = ["csv_gen.cpp", "io/csvw.cpp", "io/csvr.cpp", "utility/color.cpp", "utility/common_utils.cpp",
+               "utility/numerics.cpp"]
+
+
 def build_oracle(model, force=False):
     """Compile the restatement for one model (needs the model headers)."""
     out = oracle_lib_path(model)
@@ -132,6 +141,9 @@ def build_ref(model, force=False, cli=True):
             obj = _ezxml_obj()
             srcs = [os.path.join(srcdir, s) for s in REF_COMMON + REF_CLI_EXTRA]
             _run(["g++"] + REF_FLAGS + inc + srcs + [obj, "-o", exe])
+        exe = ref_csv_gen_path(model)
+        if force or not os.path.exists(exe):
+            _run(["g++"] + REF_FLAGS + inc + [os.path.join(srcdir, s) for s in REF_CSV_GEN] + ["-o", exe])
     return lib
 
 

@@ -108,3 +108,29 @@ def test_plan_kernels_and_bytes():
     off, ids = tissue.default_graph(200, 4)
     with pytest.raises(DenseError):
         plan("her_model_2014", [ParameterSet(off, ids, p, duration=10, mem_block=48)], 0.01, 1.0)
+
+
+@pytest.mark.parametrize("model", ["her_model_2014", "turing", "nan_test", "delay_reaction", "bz",
+                                   "briggs_rauscher"])
+def test_csv_gen_matches_dense(model, tmp_path):
+    """The drop-in csv_gen writes the same three template files, byte for
+    byte, and the same console text as DENSE's csv_gen built from source."""
+    import subprocess
+    from dense_b200.build import build_csv_gen
+    from oracle.build import ref_csv_gen_path
+    ref = ref_csv_gen_path(model)
+    if not os.path.exists(ref):
+        pytest.skip("DENSE's csv_gen not built here")
+    ours = build_csv_gen(model)
+    outs = {}
+    for name, exe in (("ref", ref), ("ours", ours)):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([exe, str(d) + "/"], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 0
+        outs[name] = (r.stdout.replace(str(d), "DIR"),
+                      {f: (d / f).read_bytes() for f in ("param_sets_template.csv", "param_pert_template.csv",
+                                                          "param_grad_template.csv")})
+    assert outs["ours"] == outs["ref"]
+    r = subprocess.run([ours], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "Missing required command line argument" in r.stdout
