@@ -139,11 +139,13 @@ def targets(F):
     return np.nan_to_num(T).astype(np.float32), M.astype(np.float32)
 
 
-def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None):
+def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, group=None, device=0):
+    """The MLP surrogate on (P, F); with a process group, data-parallel over
+    the ranks' shards (gradients averaged every step)."""
     from .surrogate import MLP
     X = encode(P)
     T, M = targets(F)
-    net = MLP(X.shape[1], T.shape[1], seed=seed, lr=lr)
+    net = MLP(X.shape[1], T.shape[1], seed=seed, lr=lr, group=group, device=device)
     net.fit(X, T, M, epochs=epochs, batch=min(batch, (X.shape[0] // 128) * 128), seed=seed, log=log)
     return net
 
@@ -205,6 +207,50 @@ def screened_search(net, n_candidates, seed, keep=0.01, plain_sample=4096, sim_k
         "accepted_period_error_median": float(np.median(per_err)) if acc_s.any() else None,
         "accepted_amplitude_error_median": float(np.median(amp_err)) if acc_s.any() else None,
     }
+
+
+def _draw_rows(rng, m, spread=SPREAD):
+    t = template()
+    return t[None, :] * np.exp(rng.uniform(np.log(1.0 / spread), np.log(spread), size=(m, t.size)))
+
+
+def screened_search_sharded(net, n_candidates, seed, keep=0.01, group=None, sim_kwargs=None, log=None):
+    """Surrogate-screened search over GPUs (one process per GPU): each rank
+    draws and scores its contiguous share of the candidates (chunked seeded
+    streams, dense_b200.distributed), the global top `keep` fraction is
+    merged from the ranks' local tops, each rank re-simulates every
+    world-th of it in FP64, and the accepted counts are summed.  Returns the
+    totals (the same on every rank); times are the max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from . import distributed as D
+    sim_kwargs = sim_kwargs or {}
+    on = dist.is_available() and dist.is_initialized()
+    rank = dist.get_rank(group) if on else 0
+    world = dist.get_world_size(group) if on else 1
+    lo, hi = D.shard_range(n_candidates, rank, world)
+    t0 = time.perf_counter()
+    P = D.candidate_range(lo, hi, seed, _draw_rows)
+    score = predicted_score(net.predict(encode(P))) if len(P) else np.zeros(0)
+    top = D.global_top(score, np.arange(lo, hi), max(1, int(round(keep * n_candidates))), group)
+    t_infer = time.perf_counter() - t0
+    mine = top[rank::world]
+    Fs = simulate_features(D.candidates_at(mine, seed, _draw_rows), log=log, **sim_kwargs) if len(mine) else None
+    acc = int(accepted(Fs).sum()) if Fs is not None else 0
+    sim_s = Fs["seconds"] if Fs is not None else 0.0
+    vals = torch.tensor([float(acc), t_infer, sim_s], dtype=torch.float64)
+    if on:
+        if dist.get_backend(group) == "nccl":
+            vals = vals.cuda()
+        s = vals[:1].clone()
+        dist.all_reduce(s, op=dist.ReduceOp.SUM, group=group)
+        m = vals[1:].clone()
+        dist.all_reduce(m, op=dist.ReduceOp.MAX, group=group)
+        vals = torch.cat([s, m]).cpu()
+    acc_total, t_inf, t_sim = float(vals[0]), float(vals[1]), float(vals[2])
+    return {"candidates": n_candidates, "ranks": world, "kept": int(len(top)), "accepted_screened": int(acc_total),
+            "inference_s": t_inf, "resimulation_s": t_sim,
+            "accepted_per_s_screened": acc_total / max(1e-12, t_inf + t_sim)}
 
 
 class SRES:

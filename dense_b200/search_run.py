@@ -14,10 +14,19 @@
 Prints one JSON object.  Usage:
   python -m dense_b200.search_run [--train N] [--test N] [--candidates N]
       [--minutes M] [--cells C] [--epochs E] [--generations G]
+
+Under torchrun (one process per GPU) steps 1, 2 and 4 shard: each rank
+simulates its share of the training candidates, the surrogate trains
+data-parallel (gradients averaged each step over NCCL), and the screening
+scores each rank's share of the candidates, merges the global top 1% and
+re-simulates it spread over the ranks (dense_b200.distributed); the
+candidates then come from chunked seeded streams; the plain-search
+baseline and SRES stay single-GPU (rank 0 reports).
 """
 
 import argparse
 import json
+import os
 import sys
 import time
 
@@ -40,6 +49,8 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=100)
     a = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        return sharded(a, log)
     sim = dict(minutes=a.minutes, cells=a.cells, width=4)
     res = {"config": vars(a)}
     t0 = time.perf_counter()
@@ -70,6 +81,37 @@ def main(argv=None):
             res["sres_" + name] = {"best_fitness_per_generation": best, "simulations": es.evaluations}
     res["total_s"] = time.perf_counter() - t0
     print(json.dumps(res))
+
+
+def sharded(a, log):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from . import distributed as D
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    rank, world = dist.get_rank(), dist.get_world_size()
+    sim = dict(minutes=a.minutes, cells=a.cells, width=4, device=local)
+    res = {"config": vars(a), "ranks": world}
+    t0 = time.perf_counter()
+    lo, hi = D.shard_range(a.train, rank, world)
+    P = D.candidate_range(lo, hi, a.seed, S._draw_rows)
+    F = S.simulate_features(P, log=log if rank == 0 else None, **sim)
+    t = torch.tensor([F["seconds"]], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    res["data"] = {"train_sets": a.train, "seconds_max_over_ranks": float(t.item())}
+    t1 = time.perf_counter()
+    net = S.train_surrogate(P, F, epochs=a.epochs, batch=2048, seed=a.seed, log=log if rank == 0 else None,
+                            group=dist.group.WORLD, device=local)
+    res["training_s"] = time.perf_counter() - t1
+    res["search"] = S.screened_search_sharded(net, a.candidates, a.seed + 2, keep=a.keep,
+                                              group=dist.group.WORLD, sim_kwargs=sim,
+                                              log=log if rank == 0 else None)
+    res["total_s"] = time.perf_counter() - t0
+    if rank == 0:
+        print(json.dumps(res))
+    dist.destroy_process_group()
 
 
 if __name__ == "__main__":

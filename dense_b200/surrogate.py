@@ -135,7 +135,10 @@ class MLP:
     rows (the padding weights stay zero: their gradients are zero).
     """
 
-    def __init__(self, n_in, n_out, seed=0, device=0, lr=1e-3):
+    def __init__(self, n_in, n_out, seed=0, device=0, lr=1e-3, group=None):
+        """`group`: a torch.distributed process group for data-parallel
+        training (every rank the same seed, so the same initial weights; the
+        gradients of each step are averaged over the ranks)."""
         import torch
         assert n_in <= IN_PAD and n_out <= OUT_PAD
         self.torch = torch
@@ -159,6 +162,7 @@ class MLP:
         self.vb = [torch.zeros_like(b) for b in self.b]
         self.steps = 0
         self._bufs = {}
+        self.group = group
 
     def _buf(self, name, shape, dtype=None):
         t = self._bufs.get(name)
@@ -252,6 +256,9 @@ class MLP:
 
     def step(self, X, T, mask):
         loss, dW, db = self.gradients(X, T, mask)
+        if self.group is not None:
+            from .distributed import average_
+            average_(dW + db, self.group)
         self.steps += 1
         for i in range(4):
             self.k.adam(self.W[i], dW[i], self.mW[i], self.vW[i], self.lr, self.steps)
@@ -263,12 +270,18 @@ class MLP:
         from lr down to lr/100 over the run."""
         rng = np.random.Generator(np.random.PCG64(seed))
         n = X.shape[0]
+        if self.group is not None:
+            # every rank takes the same number of steps: the smallest shard's
+            import torch.distributed as dist
+            t = self.torch.tensor([n], device=self.dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
+            n = int(t.item())
         hist = []
         lr0 = self.lr
         per_epoch = max(1, n // batch)
         total = epochs * per_epoch
         for ep in range(epochs):
-            order = rng.permutation(n)
+            order = rng.permutation(X.shape[0])[:n]
             tot = 0.0
             for j, s in enumerate(range(0, n - batch + 1, batch)):
                 if cosine:

@@ -119,3 +119,21 @@ def test_synchrony_known_answers():
     assert abs(synchrony(same) - 1.0) < 1e-12
     anti = np.concatenate([np.sin(t), -np.sin(t)], 1)
     assert abs(synchrony(anti) + 1.0) < 1e-12
+
+
+def test_sharded_screening_single_rank_matches_direct_resimulation():
+    """The multi-GPU screening path on one process: the top k of the scored
+    candidate range, re-simulated, gives the accepted count a direct
+    simulation of the same candidates gives."""
+    from dense_b200 import distributed as D
+    from dense_b200 import search as S
+    from dense_b200.surrogate import MLP
+    net = MLP(len(S.active_params()), 5, seed=3)
+    sim = dict(minutes=20.0, cells=40, width=4)
+    r = S.screened_search_sharded(net, 3000, seed=11, keep=0.01, sim_kwargs=sim)
+    assert r["kept"] == 30 and r["ranks"] == 1
+    P = D.candidate_range(0, 3000, 11, S._draw_rows)
+    score = S.predicted_score(net.predict(S.encode(P)))
+    _, top = D.local_top(score, np.arange(3000), 30)
+    F = S.simulate_features(D.candidates_at(top, 11, S._draw_rows), **sim)
+    assert r["accepted_screened"] == int(S.accepted(F).sum())
