@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "umma_gemm.cuh"
 
@@ -114,15 +115,73 @@ int grid_for(int64_t n) {
   return static_cast<int>(g < 4096 ? (g > 0 ? g : 1) : 4096);
 }
 
-}  // namespace
-
 // D = A . B^T (+ bias, GELU -> H) on the tensor cores; see umma_gemm.cuh
 // for the shape rules.  err (device int) collects kErr* bits.
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
+// (no link against the driver library); null when unavailable.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// Tensor map of a row-major BF16 matrix [rows][k] (leading dimension ld)
+// read in boxes of {8 K-elements, box_rows rows}, no swizzle.
+bool bf16_map(CUtensorMap* m, const void* base, int rows, int k, int ld, int box_rows) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(k), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
+  const cuuint32_t box[2] = {8, static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t elem[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, elem,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int EPI>
+cudaError_t launch_tma(const CUtensorMap& ma, const CUtensorMap& mb, float* D, int ldd, int M, int N, int K,
+                       const float* bias, __nv_bfloat16* h, int ldh, int* err, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(umma_gemm_tma_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       100 * 1024);
+  if (e != cudaSuccess) return e;
+  umma_gemm_tma_kernel<EPI><<<M / kTileM, kGemmThreads, umma_gemm_tma_smem(N), s>>>(ma, mb, D, ldd, M, N, K, bias,
+                                                                                     h, ldh, err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
 MLP_API int dense_mlp_gemm(const void* A, int lda, const void* B, int ldb, float* D, int ldd, int M, int N, int K,
                            int epilogue, const float* bias, void* H, int ldh, int* err, void* stream) {
   if ((M % kTileM) || (N % 16) || N < 16 || N > 256 || (K % kChunkK) || (lda % 8) || (ldb % 8) || (ldd % 4) ||
-      (epilogue == kEpiBiasGelu && (ldh % 8)))
+      (epilogue == kEpiBiasGelu && (ldh % 8)) || epilogue < kEpiStore || epilogue > kEpiBias)
     return 1;
+  {
+    // operands through the Tensor Memory Accelerator when its maps can be made
+    CUtensorMap ma, mb;
+    if ((reinterpret_cast<uintptr_t>(A) % 16) == 0 && (reinterpret_cast<uintptr_t>(B) % 16) == 0 &&
+        bf16_map(&ma, A, M, K, lda, kTileM) && bf16_map(&mb, B, N, K, ldb, N)) {
+      cudaStream_t s = static_cast<cudaStream_t>(stream);
+      auto* h = static_cast<__nv_bfloat16*>(H);
+      const cudaError_t e =
+          epilogue == kEpiStore      ? launch_tma<kEpiStore>(ma, mb, D, ldd, M, N, K, bias, h, ldh, err, s)
+          : epilogue == kEpiBiasGelu ? launch_tma<kEpiBiasGelu>(ma, mb, D, ldd, M, N, K, bias, h, ldh, err, s)
+                                     : launch_tma<kEpiBias>(ma, mb, D, ldd, M, N, K, bias, h, ldh, err, s);
+      return e == cudaSuccess ? 0 : 2;
+    }
+  }
   const size_t smem = umma_gemm_smem(N);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const auto* a = static_cast<const __nv_bfloat16*>(A);
