@@ -324,9 +324,25 @@ __device__ __forceinline__ void osc_check(const OscRef& o, OscQueue& q, const do
   if (q.current < 0 || q.live <= 0) return;
   const double mid = win[static_cast<size_t>(q.current) * m];
   if (!q.ext_valid) {
+    // rescan in queue order; the loads of eight entries are issued before
+    // they are folded, so their latencies overlap
     long idx = q.start;
     double hi = win[static_cast<size_t>(idx) * m], lo = hi;
-    for (long k = 1; k < q.live; ++k) {
+    long k = 1;
+    for (; k + 8 <= q.live; k += 8) {
+      double x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        idx = (idx == w - 1) ? 0 : idx + 1;
+        x[u] = win[static_cast<size_t>(idx) * m];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        hi = (hi < x[u]) ? x[u] : hi;
+        lo = (x[u] < lo) ? x[u] : lo;
+      }
+    }
+    for (; k < q.live; ++k) {
       idx = (idx == w - 1) ? 0 : idx + 1;
       const double x = win[static_cast<size_t>(idx) * m];
       hi = (hi < x) ? x : hi;
