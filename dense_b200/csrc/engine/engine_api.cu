@@ -941,10 +941,12 @@ int dense_engine_read_state(dense_engine* e, int set, double* out) {
     CUDA_TRY(cudaMemcpy(out, static_cast<double*>(e->d_state.p) + d.cell_base * 2 * NUM_SPECIES,
                         sizeof(double) * cnt, cudaMemcpyDeviceToHost));
   } else {
-    std::vector<float> tmp(cnt);
+    // FP32: the Kahan-compensated value, state minus its compensation term
+    // (the term follows the state in the set's block), in double
+    std::vector<float> tmp(2 * cnt);
     CUDA_TRY(cudaMemcpy(tmp.data(), static_cast<float*>(e->d_state.p) + d.cell_base * 2 * NUM_SPECIES,
-                        sizeof(float) * cnt, cudaMemcpyDeviceToHost));
-    for (size_t i = 0; i < cnt; ++i) out[i] = tmp[i];
+                        sizeof(float) * 2 * cnt, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < cnt; ++i) out[i] = static_cast<double>(tmp[i]) - static_cast<double>(tmp[cnt + i]);
   }
   return DENSE_OK;
 }

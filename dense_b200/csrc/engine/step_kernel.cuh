@@ -447,8 +447,12 @@ struct SmemVals {
 template <typename T>
 struct RingVals {
   T* const* rows;  // lag-0 row of each observed species (shared)
+  T* const* comp;  // FP32 Kahan: compensation row of each observed species (shared), else null
   __device__ __forceinline__ double operator()(int slot, int cell) const {
-    return static_cast<double>(rows[slot][cell]);
+    // with Kahan compensation the analyses see the compensated value,
+    // state minus its running error, in double
+    const double v = static_cast<double>(rows[slot][cell]);
+    return comp ? v - static_cast<double>(comp[slot][cell]) : v;
   }
 };
 
@@ -633,7 +637,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
 #pragma unroll
       for (int sp = 0; sp < kNS; ++sp) {
         const int row = a.val_slot[sp];
-        if (row >= 0) s_vals[row * blk + c] = static_cast<double>(cur[sp]);
+        if (row >= 0)
+          s_vals[row * blk + c] = static_cast<double>(cur[sp]) - (kKahan ? static_cast<double>(comp[sp]) : 0.0);
       }
       __syncthreads();
       const bool bad = analyses_sample(a, anl, SmemVals{s_vals, blk}, c, c, n + blk, n, age, s_samples);
@@ -770,6 +775,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
   __shared__ double s_samples[kMaxAnalyses];
   __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
   __shared__ T* s_rows[kNS];
+  __shared__ T* s_crows[kNS];
 
   const int set = set_list[blockIdx.x];
   const SetDesc& sd = a.sets[set];
@@ -818,10 +824,14 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
     if (a.n_analyses > 0) {
       for (int i = tid; i < kNS; i += blk) {
         const int row = a.val_slot[i];
-        if (row >= 0) s_rows[row] = ring + s_roff[i] + static_cast<int64_t>(step & s_mask[i]) * n;
+        if (row >= 0) {
+          s_rows[row] = ring + s_roff[i] + static_cast<int64_t>(step & s_mask[i]) * n;
+          s_crows[row] = comp_base + static_cast<int64_t>(i) * n;
+        }
       }
       __syncthreads();
-      const bool bad = analyses_sample(a, anl, RingVals<T>{s_rows}, tid, tid, blk, n, age, s_samples);
+      const bool bad =
+          analyses_sample(a, anl, RingVals<T>{s_rows, kKahan ? s_crows : nullptr}, tid, tid, blk, n, age, s_samples);
       if (bad) atomicOr(&s_flags, 1);
       __syncthreads();
       if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
@@ -1048,6 +1058,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
   __shared__ double s_samples[kMaxAnalyses];
   __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
   __shared__ T* s_rows[kNS];
+  __shared__ T* s_crows[kNS];
   __shared__ T s_rc[kWaveMaxNbrs + 1];  // RN(1 / count)
 
   const int set = set_list[blockIdx.x];
@@ -1149,10 +1160,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
     if (a.n_analyses > 0) {
       for (int i = tid; i < kNS; i += blk) {
         const int row = a.val_slot[i];
-        if (row >= 0) s_rows[row] = s_base[i] + static_cast<int64_t>(step % s_D[i]) * n;
+        if (row >= 0) {
+          s_rows[row] = s_base[i] + static_cast<int64_t>(step % s_D[i]) * n;
+          s_crows[row] = comp_base + static_cast<int64_t>(i) * n;
+        }
       }
       __syncthreads();
-      const bool bad = analyses_sample(a, anl, RingVals<T>{s_rows}, tid, tid, blk, n, age, s_samples);
+      const bool bad =
+          analyses_sample(a, anl, RingVals<T>{s_rows, kKahan ? s_crows : nullptr}, tid, tid, blk, n, age, s_samples);
       if (bad) atomicOr(&s_flags, 1);
       __syncthreads();
       if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
