@@ -220,3 +220,54 @@ def test_other_models_bitwise_vs_oracle(model):
     spec = [(E.ParameterSet(off, ids, p, init_conc=ic, duration=4.0), np.tile(p, (24, 1)))]
     an = [E.Analysis.basic(list(range(L.num_species)), 0, 24)]
     _assert_same(_oracle_vs_engine(model, spec, 0.01, 0.1, an), an)
+
+
+@pytest.mark.parametrize("cells,width", [(1, 1), (2, 1), (5, 4), (3, 3)])
+def test_tiny_and_ragged_tissues_bitwise(cells, width):
+    """Tissues of one to five cells, widths that do not divide the cell
+    count: same states and analyses as the oracle."""
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    p = workloads.log_uniform_params(1, seed=cells)[0]
+    off, ids = default_graph(cells, width)
+    spec = [(E.ParameterSet(off, ids, p, duration=6.0), np.tile(p, (cells, 1)))]
+    an = [E.Analysis.basic(["mh1", "pd"], 0, cells),
+          E.Analysis.oscillation(["mh1"], 0, cells, 0.0, float("inf"), 1.0, 0.1)]
+    _assert_same(_oracle_vs_engine("her_model_2014", spec, 0.01, 0.1, an), an)
+
+
+def test_cells_without_neighbours_bitwise():
+    """Cells with an empty neighbour list (DENSE averages 0 / 0 = NaN and
+    reads 0) next to connected ones."""
+    from dense_b200 import workloads
+    p = workloads.log_uniform_params(1, seed=21)[0]
+    nbrs = [[], [2], [1, 3], [], [0, 1, 2, 3, 5], [4]]
+    off = np.cumsum([0] + [len(x) for x in nbrs]).astype(np.int32)
+    ids = np.array([v for x in nbrs for v in x], np.int32)
+    spec = [(E.ParameterSet(off, ids, p, duration=6.0), np.tile(p, (6, 1)))]
+    an = [E.Analysis.basic(["pd", "mh1"], 0, 6)]
+    _assert_same(_oracle_vs_engine("her_model_2014", spec, 0.01, 0.1, an), an)
+
+
+def test_fp32_kahan_turing_close_to_fp64():
+    """FP32 with Kahan-compensated state in the wave kernel (in-order
+    neighbour reads), against FP64: 16 x 16 and 48 x 48 grids, 3 minutes."""
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    p = workloads.template_params("turing")
+    ic = np.array(workloads.templates()["turing"]["init_conc"])
+    sets = []
+    for N in (16, 48):
+        off, ids = default_graph(N * N, N)
+        sets.append(E.ParameterSet(off, ids, p, init_conc=ic, duration=3.0))
+    res = {}
+    for prec in (E.FP64, E.FP32_KAHAN):
+        b = E.Batch("turing", sets, 0.01, 0.1, precision=prec)
+        b.run()
+        b.sync()
+        assert (b.status() == 0).all()
+        res[prec] = [b.state(i) for i in range(len(sets))]
+        b.close()
+    for a, f in zip(res[E.FP64], res[E.FP32_KAHAN]):
+        rel = np.max(np.abs(a - f) / np.maximum(np.abs(a), 1e-3))
+        assert rel < 1e-4, rel
