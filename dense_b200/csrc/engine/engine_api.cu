@@ -171,6 +171,7 @@ struct dense_engine {
   size_t smem = 0;
   int64_t total_cell_steps = 0;
   int64_t device_bytes = 0;
+  int64_t anl_block = 0;  // doubles of analysis state per set
   std::vector<SetDesc> sets;
   std::vector<AnalysisDesc> analyses;
   std::vector<int> init_status;
@@ -593,6 +594,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
     d.nbr_base = static_cast<int64_t>(off_all.size());
     d.ring_base = ring_total;
     d.anl_base = anl_block * s;
+    e->anl_block = anl_block;
     const int e0 = static_cast<int>(idx_all.size());
     for (int c = 0; c <= n; ++c) off_all.push_back(e0 + in.nbr_offsets[c]);
     idx_all.insert(idx_all.end(), in.nbr_ids, in.nbr_ids + in.nbr_offsets[n]);
@@ -1034,6 +1036,64 @@ int dense_engine_read_trajectory(dense_engine* e, int analysis, int set, double*
   if (n > 0 && times) CUDA_TRY(cudaMemcpy(times, st + 2, sizeof(double) * n, cudaMemcpyDeviceToHost));
   if (n > 0 && values)
     CUDA_TRY(cudaMemcpy(values, st + 2 + A.range_steps, sizeof(double) * per * n, cudaMemcpyDeviceToHost));
+  return DENSE_OK;
+}
+
+// Every set's Oscillation results at once, [sets][species][cells]: one
+// strided copy per field.
+int dense_engine_read_oscillation_all(dense_engine* e, int analysis, double* amps, double* periods) {
+  if (!e || analysis < 0 || analysis >= static_cast<int>(e->analyses.size()))
+    return fail(DENSE_ERR_INVALID, "bad analysis index");
+  const AnalysisDesc& A = e->analyses[analysis];
+  if (A.kind != kOscillation) return fail(DENSE_ERR_INVALID, "analysis kind mismatch");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  const size_t k = static_cast<size_t>(A.cmax - A.cmin) * A.nsp;
+  const double* base = static_cast<const double*>(e->d_anl.p) + A.off + 2;
+  const int fields[2] = {kOscAmp, kOscPer};
+  double* outs[2] = {amps, periods};
+  for (int f = 0; f < 2; ++f) {
+    if (!outs[f] || k == 0) continue;
+    CUDA_TRY(cudaMemcpy2D(outs[f], k * sizeof(double), base + fields[f] * k, e->anl_block * sizeof(double),
+                          k * sizeof(double), e->num_sets, cudaMemcpyDeviceToHost));
+  }
+  return DENSE_OK;
+}
+
+// Every set's recorded Trajectory values, [sets][capacity][species][cells]
+// (capacity from dense_engine_trajectory_capacity), into dst -- device
+// memory when on_device, else host -- and each set's sample count.
+int dense_engine_copy_trajectory(dense_engine* e, int analysis, void* dst, int on_device, int* samples,
+                                 void* stream) {
+  if (!e || analysis < 0 || analysis >= static_cast<int>(e->analyses.size()))
+    return fail(DENSE_ERR_INVALID, "bad analysis index");
+  const AnalysisDesc& A = e->analyses[analysis];
+  if (A.kind != kTrajectory) return fail(DENSE_ERR_INVALID, "analysis kind mismatch");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  const double* st = static_cast<const double*>(e->d_anl.p) + A.off;
+  const size_t width = sizeof(double) * static_cast<size_t>(A.range_steps) * A.nsp * (A.cmax - A.cmin);
+  const size_t pitch = sizeof(double) * e->anl_block;
+  if (dst && width > 0)
+    CUDA_TRY(cudaMemcpy2DAsync(dst, width, st + 2 + A.range_steps, pitch, width, e->num_sets,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               static_cast<cudaStream_t>(stream)));
+  if (samples) {
+    std::vector<double> cnt(e->num_sets);
+    CUDA_TRY(cudaMemcpy2D(cnt.data(), sizeof(double), st, pitch, sizeof(double), e->num_sets,
+                          cudaMemcpyDeviceToHost));
+    for (int i = 0; i < e->num_sets; ++i) samples[i] = std::min(static_cast<int>(cnt[i]), A.range_steps);
+  }
+  CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  return DENSE_OK;
+}
+
+int dense_engine_trajectory_capacity(dense_engine* e, int analysis, int* capacity) {
+  if (!e || !capacity || analysis < 0 || analysis >= static_cast<int>(e->analyses.size()))
+    return fail(DENSE_ERR_INVALID, "bad analysis index");
+  const AnalysisDesc& A = e->analyses[analysis];
+  if (A.kind != kTrajectory) return fail(DENSE_ERR_INVALID, "analysis kind mismatch");
+  *capacity = A.range_steps;
   return DENSE_OK;
 }
 

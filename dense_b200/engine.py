@@ -72,6 +72,9 @@ _FUNCS = {
     "dense_engine_plan": (C.c_int, [C.POINTER(_RunDesc), C.c_int, C.POINTER(_SetDesc), C.POINTER(C.c_int64), _I,
                                     _I]),
     "dense_engine_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "dense_engine_read_oscillation_all": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "dense_engine_copy_trajectory": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, _I, C.c_void_p]),
+    "dense_engine_trajectory_capacity": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "dense_graph_capture": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, C.c_int,
                                       C.POINTER(C.c_void_p)]),
     "dense_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -257,6 +260,7 @@ class Batch:
         self.sets = list(sets)
         self.analyses = list(analyses)
         self.precision = precision
+        self.device = device
         L = self.L
         run, cset, self._keep = _describe(L, self.sets, self.analyses, step_size, analysis_interval, precision,
                                           device)
@@ -338,6 +342,29 @@ class Batch:
         self.L._check(self.L.lib.dense_engine_read_trajectory(self.h, analysis, set_index, _dp(times), _dp(vals),
                                                               k.value, C.byref(k)))
         return times, vals
+
+    def oscillation_all(self, analysis):
+        """Every set's amplitudes and periods, [sets][species][cells]."""
+        a = self.analyses[analysis]
+        shape = (len(self.sets), len(a.species), a.cell_end - a.cell_start)
+        amps, pers = np.zeros(shape), np.zeros(shape)
+        self.L._check(self.L.lib.dense_engine_read_oscillation_all(self.h, analysis, _dp(amps), _dp(pers)))
+        return amps, pers
+
+    def trajectory_device(self, analysis):
+        """Every set's recorded trajectory as a CUDA tensor [sets][capacity]
+        [species][cells] (float64, device to device) and each set's sample
+        count (numpy)."""
+        import torch
+        a = self.analyses[analysis]
+        cap = C.c_int()
+        self.L._check(self.L.lib.dense_engine_trajectory_capacity(self.h, analysis, C.byref(cap)))
+        out = torch.empty((len(self.sets), cap.value, len(a.species), a.cell_end - a.cell_start),
+                          dtype=torch.float64, device="cuda:%d" % self.device)
+        cnt = np.zeros(len(self.sets), np.int32)
+        self.L._check(self.L.lib.dense_engine_copy_trajectory(self.h, analysis, C.c_void_p(out.data_ptr()), 1,
+                                                              _ip(cnt), None))
+        return out, cnt
 
     def info(self):
         cs = C.c_int64()

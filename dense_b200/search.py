@@ -80,6 +80,28 @@ def synchrony(traj):
     return float(((s * s).sum() - n) / (n * (n - 1)))
 
 
+def synchrony_batch(X, counts):
+    """synchrony() of every set at once on the GPU: X [sets][samples][cells]
+    (a CUDA tensor; rows past a set's count are ignored), counts [sets];
+    float64, numpy array out."""
+    import torch
+    B, T, Cn = X.shape
+    cnt = torch.as_tensor(np.asarray(counts), device=X.device, dtype=torch.float64)
+    w = (torch.arange(T, device=X.device)[None, :] < cnt[:, None]).to(X.dtype)[:, :, None]
+    mean = (X * w).sum(1, keepdim=True) / cnt.clamp(min=1)[:, None, None]
+    x = (X - mean) * w
+    nrm = torch.sqrt((x * x).sum(1))                                    # [B, C]
+    top = (X.abs() * w).amax(dim=(1, 2))                                 # [B]
+    ok = nrm > 1e-12 * (1.0 + top[:, None])
+    n = ok.sum(1).to(X.dtype)
+    z = torch.where(ok[:, None, :], x / torch.where(ok, nrm, torch.ones_like(nrm))[:, None, :],
+                    torch.zeros_like(x))
+    s = z.sum(2)                                                         # [B, T]
+    syn = ((s * s).sum(1) - n) / (n * (n - 1)).clamp(min=1)
+    syn = torch.where(n >= 2, syn, torch.full_like(syn, float("nan")))
+    return syn.cpu().numpy()
+
+
 def simulate_features(P, minutes=120.0, cells=200, width=4, window=60.0, batch=4096, device=0,
                       precision=E.FP64, log=None):
     """Simulates every row of P (one set each) and returns its features."""
@@ -100,16 +122,19 @@ def simulate_features(P, minutes=120.0, cells=200, width=4, window=60.0, batch=4
         b.sync()
         st = b.status()
         cell_steps += b.info()["total_cell_steps"]
-        for i in range(len(rows)):
-            o = b.oscillation(0, i)
-            with np.errstate(invalid="ignore"):
-                per = o["pers"][0]
-                amp = o["amps"][0]
-                out["period"][s + i] = np.nanmean(per) if np.isfinite(per).any() else np.nan
-                out["amplitude"][s + i] = np.nanmean(amp) if np.isfinite(amp).any() else np.nan
-            _, vals = b.trajectory(1, i)
-            out["synchrony"][s + i] = synchrony(vals[:, 0, :])
-            out["status"][s + i] = st[i]
+        # every set's results in two strided copies and one device copy
+        amps, pers = b.oscillation_all(0)
+        with np.errstate(invalid="ignore"):
+            for key, v in (("period", pers[:, 0, :]), ("amplitude", amps[:, 0, :])):
+                # per set: the mean of the non-NaN cells, if any cell is finite
+                num = ~np.isnan(v)
+                tot = np.where(num, v, 0.0).sum(1)
+                mean = tot / np.maximum(num.sum(1), 1)
+                out[key][s:s + len(rows)] = np.where(np.isfinite(v).any(1), mean, np.nan)
+        traj, cnt = b.trajectory_device(1)
+        out["synchrony"][s:s + len(rows)] = synchrony_batch(traj[:, :, 0, :], cnt)
+        del traj
+        out["status"][s:s + len(rows)] = st
         b.close()
         if log:
             log("simulated %d / %d sets" % (min(s + batch, n), n))

@@ -188,6 +188,17 @@ DENSE_API int dense_engine_read_oscillation(dense_engine* e, int analysis, int s
 DENSE_API int dense_engine_read_trajectory(dense_engine* e, int analysis, int set, double* times, double* values,
                                            int capacity, int* samples);
 
+/* Batched reads (no counterpart in DENSE, which reads one simulation at a
+   time): every set's Oscillation amplitudes and periods, [sets][species]
+   [cells] (either pointer may be NULL); every set's recorded Trajectory
+   values, [sets][capacity][species][cells], into device memory (on_device)
+   or host memory, with each set's sample count (samples[sets], or NULL),
+   ordered on `stream`; the capacity (samples room per set). */
+DENSE_API int dense_engine_read_oscillation_all(dense_engine* e, int analysis, double* amps, double* periods);
+DENSE_API int dense_engine_copy_trajectory(dense_engine* e, int analysis, void* dst, int on_device, int* samples,
+                                           void* stream);
+DENSE_API int dense_engine_trajectory_capacity(dense_engine* e, int analysis, int* capacity);
+
 /* Batch facts: cell-steps per full run, device bytes held, history depths. */
 DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int64_t* device_bytes,
                       int* max_block_threads);

@@ -137,3 +137,49 @@ def test_sharded_screening_single_rank_matches_direct_resimulation():
     _, top = D.local_top(score, np.arange(3000), 30)
     F = S.simulate_features(D.candidates_at(top, 11, S._draw_rows), **sim)
     assert r["accepted_screened"] == int(S.accepted(F).sum())
+
+
+def test_synchrony_batch_matches_per_set():
+    """The batched GPU synchrony equals the per-set one (random traces, a
+    constant cell, sets with fewer samples than the buffer holds)."""
+    import torch
+    from dense_b200.search import synchrony, synchrony_batch
+    rng = np.random.Generator(np.random.PCG64(4))
+    X = rng.normal(size=(6, 50, 9))
+    X[1, :, 3] = 2.5
+    X[2] = np.sin(np.linspace(0, 9, 50))[:, None] * np.ones((1, 9))
+    counts = np.array([50, 50, 50, 31, 2, 1])
+    got = synchrony_batch(torch.tensor(X, device="cuda"), counts)
+    for i in range(6):
+        want = synchrony(X[i, :counts[i]])
+        if np.isnan(want):
+            assert np.isnan(got[i])
+        else:
+            assert abs(got[i] - want) < 1e-9, (i, got[i], want)
+
+
+def test_batched_reads_match_per_set_reads():
+    """read_oscillation_all and the device trajectory copy give what the
+    per-set readers give."""
+    from dense_b200 import engine as E
+    from dense_b200 import workloads
+    from dense_b200.tissue import default_graph
+    P = workloads.log_uniform_params(5, seed=13)
+    off, ids = default_graph(40, 4)
+    sets = [E.ParameterSet(off, ids, P[i], duration=(12.0 if i != 2 else 3.0)) for i in range(5)]
+    mh1 = workloads.her_species("mh1")
+    an = [E.Analysis.oscillation(mh1, 0, 40, 0.0, 10.0, 2.0, 0.1), E.Analysis.trajectory(mh1, 0, 40, 0.0, 10.0)]
+    b = E.Batch("her_model_2014", sets, 0.01, 0.1, an)
+    b.run()
+    b.sync()
+    amps, pers = b.oscillation_all(0)
+    traj, cnt = b.trajectory_device(1)
+    traj = traj.cpu().numpy()
+    for i in range(5):
+        o = b.oscillation(0, i)
+        assert np.array_equal(amps[i], o["amps"], equal_nan=True)
+        assert np.array_equal(pers[i], o["pers"], equal_nan=True)
+        _, vals = b.trajectory(1, i)
+        assert cnt[i] == vals.shape[0]
+        assert np.array_equal(traj[i, :cnt[i]], vals)
+    b.close()
