@@ -471,15 +471,17 @@ def main():
         b = E.Batch("her_model_2014", sets, 0.01, 0.1, analyses, precision=precision, device=local)
         b.run(-1)
         if analyses:
-            res = [b.oscillation(0, i) for i in range(len(sets))]
+            res = b.oscillation_all(0)          # every set's amplitudes and periods
         else:
-            res = [{"state": b.state(i)} for i in range(len(sets))]
+            res = [b.state(i) for i in range(len(sets))]
         b.close()
         barrier()
         e2e_times.append(time.perf_counter() - t0)
         if k == 0:
-            h2d = sum(s.num_cells * len(s.set_params) * 8 + s.nbr_offsets.nbytes + s.nbr_ids.nbytes for s in sets)
-            d2h = sum(sum(v.nbytes for v in r.values() if hasattr(v, "nbytes")) for r in res)
+            # parameters (one row per set, or per-cell rows), neighbour lists
+            h2d = sum(s.set_params.nbytes + (s.cell_params.nbytes if s.cell_params is not None else 0) +
+                      s.nbr_offsets.nbytes + s.nbr_ids.nbytes for s in sets)
+            d2h = sum(r.nbytes for r in res)
     e2e_s = max(e2e_times) if e2e_times else float("nan")
     if world > 1:
         x = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -522,7 +524,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": a.e2e_steps,
-                    "what": "Batch() from host arrays + full horizon + per-set oscillation results to host"},
+                    "what": "Batch() from host arrays + full horizon + every set's oscillation amplitudes and "
+                            "periods to host"},
             "gpu_launches": a.steps,
             "clocks": clk,
             "step_ms": {"min": min(step_ms), "max": max(step_ms)},
