@@ -5,7 +5,6 @@ DENSE built from its sources)."""
 
 import os
 import shlex
-import shutil
 import subprocess
 
 import pytest

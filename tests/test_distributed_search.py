@@ -4,7 +4,6 @@ the global top-k merge across two gloo ranks, and the gradient average."""
 import os
 
 import numpy as np
-import pytest
 import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp

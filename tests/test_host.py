@@ -9,7 +9,6 @@ import numpy as np
 import pytest
 
 from dense_b200 import csvio, report
-from dense_b200.build import lib_path
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

@@ -6,7 +6,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 import torch.multiprocessing as mp
 
 from dense_b200.sharding import set_cost, shard
