@@ -182,6 +182,26 @@ def predicted_score(pred):
     return pred[:, 4] - 1e-3 * np.abs(per - TARGET_PERIOD) / PERIOD_TOL
 
 
+def score_candidates(net, P, chunk=1 << 20, spread=SPREAD):
+    """predicted_score(net.predict(encode(P))) with the encoding, the
+    network and the score on the GPU, chunk by chunk; float64 numpy array."""
+    import torch
+    dev = net.dev
+    t = template()
+    idx = active_params()
+    tt = torch.as_tensor(t[idx], device=dev, dtype=torch.float64)
+    it = torch.as_tensor(idx, device=dev)
+    out = []
+    for s in range(0, P.shape[0], chunk):
+        # whole rows across (a contiguous slice, no host copy), columns picked on the GPU
+        x = torch.as_tensor(P[s:s + chunk], device=dev)[:, it]
+        x = (torch.log(x / tt) / math.log(spread)).to(torch.float32)
+        y = net.predict_device(x).to(torch.float64)
+        per = torch.exp(torch.clamp(y[:, 0], -10, 10))
+        out.append((y[:, 4] - 1e-3 * torch.abs(per - TARGET_PERIOD) / PERIOD_TOL).cpu().numpy())
+    return np.concatenate(out) if out else np.zeros(0)
+
+
 def feature_errors(net, P, F):
     """Relative error of predicted period and amplitude on sets that
     oscillate, against the FP64 simulation."""
@@ -203,7 +223,7 @@ def screened_search(net, n_candidates, seed, keep=0.01, plain_sample=4096, sim_k
     sim_kwargs = sim_kwargs or {}
     P = draw_candidates(n_candidates, seed)
     t0 = time.perf_counter()
-    score = predicted_score(net.predict(encode(P)))
+    score = score_candidates(net, P)
     t_infer = time.perf_counter() - t0
     top = np.argsort(-score, kind="stable")[:max(1, int(round(keep * n_candidates)))]
     Fs = simulate_features(P[top], log=log, **sim_kwargs)
@@ -256,7 +276,7 @@ def screened_search_sharded(net, n_candidates, seed, keep=0.01, group=None, sim_
     lo, hi = D.shard_range(n_candidates, rank, world)
     t0 = time.perf_counter()
     P = D.candidate_range(lo, hi, seed, _draw_rows)
-    score = predicted_score(net.predict(encode(P))) if len(P) else np.zeros(0)
+    score = score_candidates(net, P) if len(P) else np.zeros(0)
     top = D.global_top(score, np.arange(lo, hi), max(1, int(round(keep * n_candidates))), group)
     t_infer = time.perf_counter() - t0
     mine = top[rank::world]

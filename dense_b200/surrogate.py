@@ -201,6 +201,24 @@ class MLP:
         self.k.gemm(self.H[3], self.Wb[3], Y, EPI_BIAS, self.b[3])
         return Y
 
+    def predict_device(self, X, batch=65536):
+        """Outputs [B][n_out] as a CUDA float32 tensor, for inputs already
+        on the GPU (a float tensor [B][n_in]); nothing crosses to the host."""
+        torch = self.torch
+        self._cast_weights()
+        out = []
+        for s in range(0, X.shape[0], batch):
+            x = X[s:s + batch]
+            B = x.shape[0]
+            Bp = (B + 127) // 128 * 128
+            Xb = self._buf("Xb", (Bp, IN_PAD), torch.bfloat16)
+            Xb.zero_()
+            Xb[:B, :self.n_in] = x.to(torch.bfloat16)
+            Y = self.forward(Xb)
+            out.append(Y[:B, :self.n_out].clone())
+        self.k.check()
+        return torch.cat(out) if out else torch.zeros((0, self.n_out), device=self.dev)
+
     def predict(self, X, batch=65536):
         """Outputs [B][n_out] (float32, on the host)."""
         self._cast_weights()

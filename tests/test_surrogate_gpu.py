@@ -183,3 +183,18 @@ def test_batched_reads_match_per_set_reads():
         assert cnt[i] == vals.shape[0]
         assert np.array_equal(traj[i, :cnt[i]], vals)
     b.close()
+
+
+def test_device_scoring_matches_host_scoring():
+    """score_candidates (encoding, network and score on the GPU) ranks like
+    the host path predicted_score(net.predict(encode(P)))."""
+    from dense_b200 import search as S
+    from dense_b200.surrogate import MLP
+    net = MLP(len(S.active_params()), 5, seed=7)
+    P = S.draw_candidates(5000, 3)
+    host = S.predicted_score(net.predict(S.encode(P)))
+    dev = S.score_candidates(net, P, chunk=2048)
+    # float32 encodings computed on two devices: equal to rounding
+    assert np.max(np.abs(host - dev)) < 1e-4
+    top_h, top_d = set(np.argsort(-host)[:50].tolist()), set(np.argsort(-dev)[:50].tolist())
+    assert len(top_h & top_d) >= 45
