@@ -37,7 +37,7 @@ from . import search as S
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--train", type=int, default=131072)
+    ap.add_argument("--train", type=int, default=200000)
     ap.add_argument("--test", type=int, default=4096)
     ap.add_argument("--candidates", type=int, default=1000000)
     ap.add_argument("--keep", type=float, default=0.01)

@@ -103,12 +103,16 @@ def test_search_pipeline_small():
     net = S.train_surrogate(P, F, epochs=60, batch=128)
     err = S.feature_errors(net, P, F)
     assert err["period_median"] < 0.5 and err["oscillation_accuracy"] > 0.6
-    res = S.screened_search(net, 20000, 6, keep=0.01, plain_sample=200, sim_kwargs=sim)
-    assert res["kept"] == 200 and res["plain_sample"] == 200
+    res = S.screened_search(net, 20000, 6, keep=0.01, plain_sample=2000, sim_kwargs=sim)
+    assert res["kept"] == 200 and res["plain_sample"] == 2000
+    # what the network gains: the share of the kept candidates that the FP64
+    # re-simulation accepts is above the share of random candidates it accepts
+    screened_fraction = res["accepted_screened"] / res["kept"]
+    assert screened_fraction > 2.0 * res["plain_accept_fraction"], res
     fit = lambda X: S.search_fitness(S.simulate_features(S.decode(X), **sim))  # noqa: E731
     es = S.SRES(len(S.active_params()), fit, mu=4, lam=32, seed=1)
-    f0 = float(np.min(es.f))
-    assert es.step() <= f0 + 1e-12 or True
+    assert es.evaluations == 32
+    assert np.isfinite(es.step())
     assert es.evaluations == 64
 
 
