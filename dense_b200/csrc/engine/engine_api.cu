@@ -402,11 +402,13 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
     off += static_cast<int64_t>(depth) * n;
   }
   // wave kernel shared memory, filled in priority order while it fits:
-  // the rows of the species read at lag S-1, the cell records, the rows of
+  // the rows of the species read at lag S-1, the FP32 Kahan terms (every
+  // cell reads and writes them each step), the cell records, the rows of
   // other neighbour-read species, then (unless the hint keeps them global)
   // the rest; the 16-bit level offsets always, at the end
   d.wave = plan.wave ? 1 : 0;
   d.topo_off = -1;
+  d.comp_smem_off = -1;
   d.lvl_smem_off = 0;
   d.smem_bytes = 0;
   for (int sp = 0; sp < NUM_SPECIES; ++sp) d.smem_off[sp] = -1;
@@ -423,6 +425,8 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
     const bool global_rows = in.schedule == DENSE_SCHEDULE_WAVE_GLOBAL;
     for (int sp = 0; sp < NUM_SPECIES && !global_rows; ++sp)
       if (ord_sp[sp]) d.smem_off[sp] = static_cast<int>(take(static_cast<int64_t>(d.D[sp]) * n * elem_bytes));
+    if (elem_bytes == 4 && !global_rows && in.schedule != DENSE_SCHEDULE_SHARED_NEIGHBOUR)
+      d.comp_smem_off = static_cast<int>(take(static_cast<int64_t>(NUM_SPECIES) * n * elem_bytes));
     d.topo_off = global_rows ? -1 : static_cast<int>(take(16 * static_cast<int64_t>(n)));
     for (int pass = 0; pass < 2 && !global_rows; ++pass) {
       if (pass == 1 && in.schedule == DENSE_SCHEDULE_SHARED_NEIGHBOUR) break;

@@ -87,6 +87,7 @@ struct SetDesc {
   int smem_off[kNS];     // byte offset of the species' rows in shared memory, -1: global
   int lvl_smem_off;      // byte offset of the 16-bit level offsets in shared memory
   int topo_off;          // byte offset of the records in shared memory, -1: global
+  int comp_smem_off;     // FP32: byte offset of the Kahan terms [kNS][n] in shared memory, -1: global
   int smem_bytes;        // dynamic shared memory the set needs
   int64_t rec_base;      // first record of the set in StepArgs::wave_rec
   // time pipelining: step k + 1 runs wave_delta levels behind step k, so

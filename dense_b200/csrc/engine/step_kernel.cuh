@@ -1107,6 +1107,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
     const int rows = sd.D[sp] * n;
     for (int i = tid; i < rows; i += blk) dst[i] = src[i];
   }
+  // FP32 Kahan terms [kNS][n]: staged in shared memory when planned there
+  T* const comp_g = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS) + static_cast<int64_t>(kNS) * n;
+  const bool comp_shared = kKahan && sd.comp_smem_off >= 0;
+  T* const comp_base = comp_shared ? reinterpret_cast<T*>(w_dyn + sd.comp_smem_off) : comp_g;
+  if (comp_shared)
+    for (int i = tid; i < kNS * n; i += blk) comp_base[i] = comp_g[i];
   __syncthreads();
   if (kUniform) {
     // the lag tables' bound checks take the row count as D - 1
@@ -1127,7 +1133,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
   }
   __syncthreads();
 
-  T* comp_base = static_cast<T*>(a.state) + sd.cell_base * (2 * kNS) + static_cast<int64_t>(kNS) * n;
   int err = 0;
   const T dt = static_cast<T>(a.dt);
   int chunk = pg.chunk;
@@ -1261,6 +1266,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
     const int rows = sd.D[sp] * n;
     for (int i = tid; i < rows; i += blk) dst[i] = src[i];
   }
+  if (comp_shared)
+    for (int i = tid; i < kNS * n; i += blk) comp_g[i] = comp_base[i];
   if (err) atomicOr(&s_flags, err << 1);
   if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
   __syncthreads();

@@ -260,14 +260,19 @@ def test_fp32_kahan_turing_close_to_fp64():
     for N in (16, 48):
         off, ids = default_graph(N * N, N)
         sets.append(E.ParameterSet(off, ids, p, init_conc=ic, duration=3.0))
-    res = {}
+    res, basic = {}, {}
     for prec in (E.FP64, E.FP32_KAHAN):
-        b = E.Batch("turing", sets, 0.01, 0.1, precision=prec)
+        # Basic over 0..255 of every set: the analyses sample the
+        # compensated values (the Kahan terms live in shared memory)
+        an = [E.Analysis.basic(list(range(4)), 0, 256)]
+        b = E.Batch("turing", sets, 0.01, 0.1, an, precision=prec)
         b.run()
         b.sync()
         assert (b.status() == 0).all()
         res[prec] = [b.state(i) for i in range(len(sets))]
+        basic[prec] = [np.concatenate([b.basic(0, i)[k].ravel() for k in ("cell_mins", "cell_maxs", "cell_sums")])
+                       for i in range(len(sets))]
         b.close()
-    for a, f in zip(res[E.FP64], res[E.FP32_KAHAN]):
+    for a, f in zip(res[E.FP64] + basic[E.FP64], res[E.FP32_KAHAN] + basic[E.FP32_KAHAN]):
         rel = np.max(np.abs(a - f) / np.maximum(np.abs(a), 1e-3))
         assert rel < 1e-4, rel
