@@ -129,7 +129,13 @@ typedef struct dense_run_desc {
 
 typedef struct dense_engine dense_engine;
 
+/* The compiled model's counts: NUM_SPECIES (core/specie.hpp:25),
+   NUM_REACTIONS (core/reaction.hpp:19), NUM_DELAY_REACTIONS
+   (core/reaction.hpp:29-36), NUM_CRITICAL_SPECIES (core/specie.hpp:28-35),
+   NUM_PARAMS (core/parameter_set.hpp:10). */
 DENSE_API int dense_model_get_info(dense_model_info* out);
+/* specie_str[species] (core/specie.hpp:19) and reaction_str[reaction]
+   (core/reaction.hpp:23); NULL out of range. */
 DENSE_API const char* dense_model_specie_name(int species);
 DENSE_API const char* dense_model_reaction_name(int reaction);
 /* Reaction name of delay reaction d (reactions_list.hpp order of the
@@ -137,33 +143,48 @@ DENSE_API const char* dense_model_reaction_name(int reaction);
    (specie_list.hpp order of the CRITICAL_SPECIE entries); NULL out of range. */
 DENSE_API const char* dense_model_delay_reaction_name(int d);
 DENSE_API const char* dense_model_critical_specie_name(int c);
+/* Text of the last failure on this thread (what DENSE's exceptions carry
+   in what()). */
 DENSE_API const char* dense_last_error(void);
 
-/* Validate and stage a batch on the device (host buffers are copied). */
+/* Validate and stage a batch on the device (host buffers are copied).
+   Replaces Sim_Builder::get_simulations and the Deterministic_Simulation
+   constructor per set (deterministic_main.cpp:53, sim/determ/determ.cpp:31-52)
+   and the analyses parse_analysis_entries builds (deterministic_main.cpp:54). */
 DENSE_API int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set_desc* sets,
                         dense_engine** out);
 
 /* Run the next `num_chunks` analysis chunks of every set (-1: to the end of
    each set's horizon), on `stream` (a cudaStream_t, or NULL for the
-   engine's own stream).  Sets finishing their horizon are finalized. */
+   engine's own stream).  Sets finishing their horizon are finalized.
+   Replaces run_simulation's chunk loop (run_simulation.hpp:84-165) over
+   Deterministic_Simulation::age_by (sim/determ/determ.cpp:9-21). */
 DENSE_API int dense_engine_run(dense_engine* e, int num_chunks, void* stream);
 
 /* Same, replayed from a CUDA graph captured on first use for this chunk
-   count. */
+   count (no counterpart in DENSE). */
 DENSE_API int dense_engine_run_graph(dense_engine* e, int num_chunks, void* stream);
 
+/* Wait for the engine's stream (no counterpart in DENSE, which is
+   synchronous). */
 DENSE_API int dense_engine_sync(dense_engine* e);
 
-/* Reset every set to its initial state (same inputs; no reallocation). */
+/* Reset every set to its initial state (same inputs; no reallocation; in
+   DENSE a new Simulation object). */
 DENSE_API int dense_engine_reset(dense_engine* e, void* stream);
 
-/* Per-set status words (DENSE_SET_* bits), [num_sets]. */
+/* Per-set status words (DENSE_SET_* bits), [num_sets]: the drop that
+   run_simulation makes when an analysis throws Bad_Simulation_Error
+   (run_simulation.hpp:131-150, measurement/conccheck.hpp:48), as a word. */
 DENSE_API int dense_engine_status(dense_engine* e, int32_t* out);
 
-/* Chunks done and simulated age per set, [num_sets] each. */
+/* Chunks done and simulated age per set, [num_sets] each
+   (Simulation::age, sim/base.hpp:124). */
 DENSE_API int dense_engine_progress(dense_engine* e, int32_t* chunks, double* age);
 
-/* Lag-0 concentrations of one set, [num_species][num_cells]. */
+/* Lag-0 concentrations of one set, [num_species][num_cells]:
+   Deterministic_Simulation::get_concentration(cell, species)
+   (sim/determ/determ.hpp:73-75) for every cell and species. */
 DENSE_API int dense_engine_read_state(dense_engine* e, int set, double* out);
 
 /* BasicAnalysis `analysis` of one set: mins/sums/maxs [n], per-cell
@@ -199,13 +220,17 @@ DENSE_API int dense_engine_copy_trajectory(dense_engine* e, int analysis, void* 
                                            void* stream);
 DENSE_API int dense_engine_trajectory_capacity(dense_engine* e, int analysis, int* capacity);
 
-/* Batch facts: cell-steps per full run, device bytes held, history depths. */
+/* Batch facts: cell-steps per full run, device bytes held, threads per
+   CTA of the register kernel (no counterpart in DENSE). */
 DENSE_API int dense_engine_info(dense_engine* e, int64_t* total_cell_steps, int64_t* device_bytes,
                       int* max_block_threads);
 
-/* Staged history depth (D) and DENSE ring size (S) per species of a set. */
+/* Staged history depth (D) and DENSE ring size (S) per species of a set;
+   S is baby_cl's per-species row count (sim/determ/baby_cl.cpp:10). */
 DENSE_API int dense_engine_ring_info(dense_engine* e, int set, int* S, int* D);
 
+/* Free the batch's device buffers (the simulations' destruction at the end
+   of run_simulation). */
 DENSE_API int dense_engine_destroy(dense_engine* e);
 
 /* One CUDA graph over several batches, possibly of different models (no
