@@ -92,6 +92,29 @@ def _nan_test():
                 analyses=[dict(kind="basic", species=[0, 1, 2], cells=(0, 99), t=(0.0, 2.0))])
 
 
+def _other(model, seed, delay_sets=()):
+    # DENSE's other example models (their templates hold zero rates):
+    # seeded positive rates U[0.05, 2), initial concentrations U[0, 5),
+    # 24 cells of width 6, 4 minutes; one set with delays U[0.5, 4) and one
+    # per entry of `delay_sets` (explicit delays, e.g. the template's
+    # 100-minute ones, whose reads only ever see the initial rows)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = workloads.templates()[model]
+    nsp, nr = len(t["species"]), len(t["reactions"])
+    p = rng.uniform(0.05, 2.0, size=t["num_params"])
+    nd = t["num_params"] - nr if model == "delay_reaction" else 0
+    p[nr:nr + nd] = rng.uniform(0.5, 4.0, nd)
+    ic = rng.uniform(0.0, 5.0, size=nsp)
+    sets = [_set(model, 24, 6, 4.0, set_params=p, init_conc=ic)]
+    for d in delay_sets:
+        q = p.copy()
+        q[nr:nr + nd] = d
+        sets.append(_set(model, 24, 6, 4.0, set_params=q, init_conc=ic))
+    return dict(model=model, dt=0.01, interval=0.1, sets=sets,
+                analyses=[dict(kind="basic", species=list(range(nsp)), cells=(0, 24), t=(0.0, INF)),
+                          dict(kind="oscillation", species=[0], cells=(0, 24), t=(0.0, INF), win=1.0, intvl=0.1)])
+
+
 CASES = {
     "her_test": _her_test,
     "her_pert": _her_pert,
@@ -100,6 +123,9 @@ CASES = {
     "her_init": _her_init,
     "turing": _turing,
     "nan_test": _nan_test,
+    "delay_reaction": lambda: _other("delay_reaction", 21, delay_sets=[(100.0, 100.0)]),
+    "bz": lambda: _other("bz", 22),
+    "briggs_rauscher": lambda: _other("briggs_rauscher", 23),
 }
 
 

@@ -13,7 +13,8 @@ from tests.helpers import load_fixture, mismatches, run_engine, run_oracle
 
 pytestmark = pytest.mark.gpu
 
-EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init", "turing", "nan_test"]
+EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init", "turing", "nan_test", "delay_reaction",
+               "bz", "briggs_rauscher"]
 
 
 @pytest.mark.parametrize("name", EXACT_CASES)
