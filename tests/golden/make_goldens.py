@@ -58,6 +58,29 @@ CLI_CASES = {
     "her_test": ("her_model_2014",
                  "-p {in}/her_param_sets.csv --cell-total 10 --tissue-width 5 --time-total 3000 --anlys-intvl .01 "
                  "--step-size .01 --analysis {in}/her_analyses.xml", ["anlys_basic_a.csv", "anlys_oscil.csv"]),
+    # the other her_model_2014 CTest runs (test/her_model_2014/CMakeLists.txt:20-90):
+    # tissue width, cell count and total time; with 20 or more cells the
+    # second Basic (cells 0-19) lies in the tissue and is compared too
+    "her_cell_width_test": ("her_model_2014",
+                            "--param-sets {in}/her_param_sets.csv --cell-total 10 --tissue-width 1 --time-total 3000 "
+                            "--anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                            ["anlys_basic_a.csv", "anlys_oscil.csv"]),
+    "her_cell_width_test_01": ("her_model_2014",
+                               "--param-sets {in}/her_param_sets.csv --cell-total 50 --tissue-width 10 "
+                               "--time-total 3000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                               ["anlys_basic_a.csv", "anlys_basic_b.csv", "anlys_oscil.csv"]),
+    "her_cell_number_test_01": ("her_model_2014",
+                                "--param-sets {in}/her_param_sets.csv --cell-total 200 --tissue-width 5 "
+                                "--time-total 3000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                                ["anlys_basic_a.csv", "anlys_basic_b.csv", "anlys_oscil.csv"]),
+    "her_time_total_test": ("her_model_2014",
+                            "--param-sets {in}/her_param_sets.csv --cell-total 10 --tissue-width 5 --time-total 300 "
+                            "--anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                            ["anlys_basic_a.csv", "anlys_oscil.csv"]),
+    "her_time_total_test_01": ("her_model_2014",
+                               "--param-sets {in}/her_param_sets.csv --cell-total 10 --tissue-width 5 "
+                               "--time-total 5000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                               ["anlys_basic_a.csv", "anlys_oscil.csv"]),
     "nan_test": ("nan_test",
                  "--param-sets {in}/nan_param_sets.csv --cell-total 100 --tissue-width 100 --time-total 15 "
                  "--anlys-intvl 0.5 -s 0.01 --analysis {in}/nan_analyses.xml", ["anlys_basic_a.csv"]),
