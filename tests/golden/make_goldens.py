@@ -69,6 +69,14 @@ CLI_CASES = {
                                "--param-sets {in}/her_param_sets.csv --cell-total 50 --tissue-width 10 "
                                "--time-total 3000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
                                ["anlys_basic_a.csv", "anlys_basic_b.csv", "anlys_oscil.csv"]),
+    "her_cell_width_test_02": ("her_model_2014",
+                               "--param-sets {in}/her_param_sets.csv --cell-total 100 --tissue-width 10 "
+                               "--time-total 3000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                               ["anlys_basic_a.csv", "anlys_basic_b.csv", "anlys_oscil.csv"]),
+    "her_cell_number_test": ("her_model_2014",
+                             "--param-sets {in}/her_param_sets.csv --cell-total 50 --tissue-width 5 "
+                             "--time-total 3000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
+                             ["anlys_basic_a.csv", "anlys_basic_b.csv", "anlys_oscil.csv"]),
     "her_cell_number_test_01": ("her_model_2014",
                                 "--param-sets {in}/her_param_sets.csv --cell-total 200 --tissue-width 5 "
                                 "--time-total 3000 --anlys-intvl .01 --step-size .01 --analysis {in}/her_analyses.xml",
