@@ -342,6 +342,96 @@ def run_turing(a):
     b.close()
 
 
+def run_single(a):
+    """One her_model_2014 set: 200 cells on DENSE's default tissue (-c 200
+    -w 4), every parameter of every cell x U(0.95, 1.05) (seeded), dt 0.01
+    min, 600 min, Basic over every species and cell and Oscillation of mh1
+    and ph1 every 0.1 min.  A timed step is the whole 600-minute run of the
+    set (reset before it, outside its events); one set occupies one SM, so
+    the step is bound by the latency of its 60,000 dependent Euler steps."""
+    import torch
+    from dense_b200 import engine as E, workloads
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    minutes = a.minutes if a.minutes != 1200.0 else 600.0
+    ps = workloads.perturbed_set(cells=200, width=4, duration=minutes, seed=1)
+    an = workloads.cfg1_analyses(200, 0.1)
+    b = E.Batch("her_model_2014", [ps], 0.01, 0.1, an, device=local)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    for _ in range(a.warmup):
+        b.reset(stream=sptr)
+        b.run(-1, stream=sptr)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    clocks = Clocks(local)
+    for k in range(a.steps):
+        b.reset(stream=sptr)
+        ev[k][0].record(stream)
+        b.run(-1, stream=sptr)
+        ev[k][1].record(stream)
+    stream.synchronize()
+    clk = clocks.stop()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    ms = sum(step_ms) / a.steps
+    cell_steps = b.info()["total_cell_steps"]
+    value = cell_steps / (ms / 1e3)
+    status = int((b.status() != 0).sum())
+    b.close()
+    # e2e: the public API from host arrays: create (host->device), the run,
+    # every analysis output of the set back to the host
+    e2e_s, h2d, d2h = [], 0, 0
+    for _ in range(max(1, a.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eb = E.Batch("her_model_2014", [ps], 0.01, 0.1, an, device=local)
+        eb.run(-1)
+        basic, osc = eb.basic(0, 0), eb.oscillation(1, 0)
+        eb.sync()
+        e2e_s.append(time.perf_counter() - t0)
+        eb.close()
+        h2d = ps.set_params.nbytes + ps.cell_params.nbytes + ps.nbr_offsets.nbytes + ps.nbr_ids.nbytes
+        d2h = sum(np.asarray(v).nbytes for v in list(basic.values()) + list(osc.values()))
+    cpu = None
+    if not a.no_cpu:
+        from oracle.pyoracle import load_oracle, load_ref
+        lib, kind = load_ref("her_model_2014"), "reference"
+        if lib is None:
+            lib, kind = load_oracle("her_model_2014"), "port"
+        nsp = len(workloads.templates()["her_model_2014"]["species"])
+        t0 = time.perf_counter()
+        sim = lib.create(ps.nbr_offsets, ps.nbr_ids, ps.cell_params, ps.set_params, None, 0.01)
+        sim.add_basic(list(range(nsp)), 0, 200, 0.0, float("inf"))
+        sim.add_oscillation(workloads.her_species("mh1", "ph1"), 0, 200, 0.0, float("inf"), 4.0, 0.1)
+        chunks = sim.run(minutes, 0.1)
+        secs = time.perf_counter() - t0
+        cpu = {"value": chunks * 10 * 200 / secs, "unit": "cell-steps/s", "cores": 1, "kind": kind,
+               "sample": "the whole workload (one set, %g min) on one host core, %.1f s" % (minutes, secs)}
+    hbm, peak_src = peaks()
+    achieved = BYTES_PER_CELL_STEP * value / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "her_model_2014, one set, 200 cells (-c 200 -w 4), every parameter of every cell "
+                                   "x U(0.95, 1.05), dt 0.01 min, %g min, Basic (all species and cells) + "
+                                   "Oscillation (mh1, ph1) every 0.1 min" % minutes,
+                       "step": "the whole run of the set", "l2": "one set: state and history fit in L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None,
+                         "basis": "%d algorithmic bytes per cell-step; one set runs on one SM, so the step is "
+                                  "latency-bound and far from either roofline; peak %s"
+                                  % (BYTES_PER_CELL_STEP, peak_src)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cell_steps / statistics.median(e2e_s), "unit": "cell-steps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": len(e2e_s),
+                    "what": "Batch() from host arrays + the run + every analysis output to host"},
+            "gpu_launches": a.steps, "clocks": clk,
+            "step_ms": {"min": min(step_ms), "max": max(step_ms)},
+            "status_nonzero_sets": status}), flush=True)
+
+
 def _ref_worker(args):
     seed, minutes = args
     r = cpu_sample("reference", num_sets=1, minutes=minutes, seed=seed)
@@ -394,9 +484,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--analyses", default="oscillation", choices=["oscillation", "none"],
                     help="the workload's analyses: Oscillation(mh1) every 0.1 min, or none")
-    ap.add_argument("--workload", default="batch", choices=["batch", "mixed", "turing"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "mixed", "turing", "single"],
                     help="batch: 4096 her_model_2014 sets of 200 cells; mixed: the uneven her + Turing batch "
-                         "(10000 sets unless --sets is given); turing: sets of one Turing grid (--grid)")
+                         "(10000 sets unless --sets is given); turing: sets of one Turing grid (--grid); "
+                         "single: one perturbed her_model_2014 set of 200 cells, 600 min, Basic + Oscillation")
     ap.add_argument("--grid", type=int, default=64, help="turing workload: grid side N")
     a = ap.parse_args()
     if a.impl == "reference":
@@ -405,6 +496,8 @@ def main():
         return run_mixed(a)
     if a.workload == "turing":
         return run_turing(a)
+    if a.workload == "single":
+        return run_single(a)
 
     import torch
     rank, world, local = dist_env()
