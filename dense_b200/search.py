@@ -102,9 +102,15 @@ def synchrony_batch(X, counts):
     return syn.cpu().numpy()
 
 
-def simulate_features(P, minutes=120.0, cells=200, width=4, window=60.0, batch=4096, device=0,
+def simulate_features(P, minutes=None, cells=200, width=4, window=60.0, batch=4096, device=0,
                       precision=E.FP64, log=None):
-    """Simulates every row of P (one set each) and returns its features."""
+    """Simulates every row of P (one set each) and returns its features.
+
+    Every feature is taken over [0, window), and the first `window` minutes
+    of a forward simulation do not depend on what follows, so the horizon
+    defaults to the window's end (`minutes`=None); a longer horizon gives
+    the same features at a higher cost."""
+    minutes = window if minutes is None else minutes
     off, ids = default_graph(cells, width)
     mh1 = workloads.her_species("mh1")
     n = P.shape[0]

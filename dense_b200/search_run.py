@@ -42,7 +42,7 @@ def main(argv=None):
     ap.add_argument("--candidates", type=int, default=1000000)
     ap.add_argument("--keep", type=float, default=0.01)
     ap.add_argument("--plain-sample", type=int, default=4096)
-    ap.add_argument("--minutes", type=float, default=120.0)
+    ap.add_argument("--minutes", type=float, default=60.0, help="simulated minutes (the feature window is 0-60)")
     ap.add_argument("--cells", type=int, default=200)
     ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--generations", type=int, default=3)
