@@ -284,12 +284,17 @@ int build_analyses(const dense_run_desc* run, int num_sets, const dense_set_desc
     } else if (in.kind == DENSE_ANALYSIS_TRAJECTORY) {
       // room for every sample inside [time_start, time_end) of the longest
       // horizon in the batch
+      // (sets with a negative or NaN duration are rejected by check_set)
       int cap = 0;
       for (int s = 0; s < num_sets; ++s) {
-        const double t1 = std::min(in.time_end, in_sets[s].duration), t0 = std::max(in.time_start, 0.0);
-        const int all = static_cast<int>(std::ceil(in_sets[s].duration / interval));
-        const int in_window = t1 > t0 ? static_cast<int>(std::ceil((t1 - t0) / interval)) + 2 : 0;
-        cap = std::max(cap, std::min(all, in_window));
+        const double dur = in_sets[s].duration;
+        if (!(dur >= 0.0)) continue;
+        const double t1 = std::min(in.time_end, dur), t0 = std::max(in.time_start, 0.0);
+        const double all = std::ceil(dur / interval);
+        const double in_window = t1 > t0 ? std::ceil((t1 - t0) / interval) + 2.0 : 0.0;
+        const double c = std::min(all, in_window);
+        if (!(c < 1e9)) return fail(DENSE_ERR_UNSUPPORTED, "trajectory: too many samples");
+        cap = std::max(cap, static_cast<int>(c));
       }
       A.range_steps = cap;
       anl_block += 2 + cap + static_cast<int64_t>(cap) * A.nsp * m;

@@ -1,0 +1,104 @@
+"""Error behaviour of the C ABI on malformed input, through
+dense_engine_plan (the same validation dense_engine_create runs before it
+touches a GPU): every bad descriptor is refused with its DENSE_ERR_* code
+and a message, nothing is undefined behaviour."""
+
+import numpy as np
+import pytest
+
+from dense_b200 import engine as E, workloads
+from dense_b200.tissue import default_graph
+
+INVALID, UNSUPPORTED = 1, 4
+
+
+def _set(cells=8, width=4, **kw):
+    off, ids = default_graph(cells, width)
+    kw.setdefault("duration", 10.0)
+    return E.ParameterSet(off, ids, workloads.template_params(), **kw)
+
+
+def _code(sets, analyses=(), dt=0.01, interval=0.1, precision=E.FP64):
+    try:
+        E.plan("her_model_2014", sets, dt, interval, analyses, precision)
+    except E.DenseError as e:
+        text = str(e)
+        return int(text.split("error ")[1].split(":")[0]), text
+    return 0, ""
+
+
+def _csr(offsets, ids, **kw):
+    return E.ParameterSet(np.array(offsets), np.array(ids), workloads.template_params(), duration=10.0, **kw)
+
+
+def test_a_valid_batch_plans():
+    assert _code([_set(), _set(200, 4)]) == (0, "")
+
+
+@pytest.mark.parametrize("offsets,ids,msg", [
+    ([0, 1, 2], [1, 5], "neighbour id outside the tissue"),
+    ([0, 1, 2], [1, -1], "neighbour id outside the tissue"),
+    ([0, 2, 2], [1, 1], "must ascend"),
+    ([0, 2, 1], [0, 1], "CSR offsets decrease"),
+    ([1, 2, 3], [1, 0, 0], "CSR offsets must start at 0"),
+])
+def test_bad_neighbour_lists(offsets, ids, msg):
+    code, text = _code([_csr(offsets, ids)])
+    assert code == INVALID and msg in text
+
+
+def test_cell_count_limits():
+    code, text = _code([_csr([0], [])])
+    assert code == UNSUPPORTED and "cells per set" in text
+
+
+@pytest.mark.parametrize("duration", [-1.0, float("nan")])
+def test_bad_duration(duration):
+    code, text = _code([_set(duration=duration)])
+    assert code == INVALID and "duration" in text
+
+
+@pytest.mark.parametrize("duration", [-1.0, float("nan"), 1e300])
+def test_bad_duration_with_a_trajectory(duration):
+    """The trajectory capacity is sized from the sets' horizons before the
+    sets are checked; an invalid or absurd horizon is an error code."""
+    an = [E.Analysis.trajectory(["mh1"], 0, 8)]
+    code, _ = _code([_set(), _set(duration=duration)], an)
+    assert code in (INVALID, UNSUPPORTED)
+
+
+@pytest.mark.parametrize("dt,interval", [(0.0, 0.1), (-0.01, 0.1), (0.01, 0.0), (float("nan"), 0.1)])
+def test_bad_step_or_interval(dt, interval):
+    code, text = _code([_set()], dt=dt, interval=interval)
+    assert code == INVALID and "positive" in text
+
+
+def test_unknown_precision():
+    code, text = _code([_set()], precision=7)
+    assert code == INVALID and "precision" in text
+
+
+@pytest.mark.parametrize("schedule,mem_block,msg", [
+    (5, 0, "schedule hint"), (-1, 0, "schedule hint"), (1, 48, "mem_block"), (1, 512, "mem_block"),
+    (1, 16, "mem_block"),
+])
+def test_bad_schedule_hints(schedule, mem_block, msg):
+    code, text = _code([_set(schedule=schedule, mem_block=mem_block)])
+    assert code == INVALID and msg in text
+
+
+def test_analysis_checks():
+    s = [_set(8, 4)]
+    assert _code(s, [E.Analysis.basic(["mh1"], 0, 9)])[0] == INVALID          # past the tissue
+    assert _code(s, [E.Analysis.basic(["mh1"], 5, 4)])[0] == INVALID          # end before start
+    assert _code(s, [E.Analysis.basic([14], 0, 8)])[0] == INVALID             # species id
+    assert _code(s, [E.Analysis.basic([], 0, 8)])[0] == INVALID               # no species
+    assert _code(s, [E.Analysis.oscillation(["mh1"], 0, 8, 0, 10, 4.0, 0.0)])[0] == INVALID
+    assert _code(s, [E.Analysis.oscillation(["mh1"], 0, 8, 0, 10, 1e9, 1e-3)])[0] == UNSUPPORTED
+    assert _code(s, [E.Analysis.basic(["mh1"], 0, 8)] * 9)[0] == UNSUPPORTED   # more than 8 analyses
+    assert _code(s, [E.Analysis.conccheck([], 0, 8, 0.0, 1e3)])[0] == 0     # all species
+
+
+def test_analysis_range_is_checked_against_the_smallest_set():
+    code, text = _code([_set(200, 4), _set(8, 4)], [E.Analysis.basic(["mh1"], 0, 100)])
+    assert code == INVALID and "outside the tissue" in text
