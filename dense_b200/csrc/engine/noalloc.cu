@@ -134,8 +134,6 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   const double dt = run->step_size, interval = run->analysis_interval;
   const double steps_d = interval / dt;
   if (!(steps_d < 2147483647.0)) return nfail(DENSE_ERR_INVALID, "interval / step size too large");
-  cudaError_t ce = cudaSetDevice(run->device);
-  if (ce != cudaSuccess) return nfail(DENSE_ERR_CUDA, "cudaSetDevice failed");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   // ---- plan every set on the host (stack memory only)
@@ -151,6 +149,8 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
       return nfail(DENSE_ERR_INVALID, "bad set (1..256 cells, CSR and parameters required)");
     const int n = in.num_cells;
     if (in.nbr_offsets[0] != 0) return nfail(DENSE_ERR_INVALID, "CSR offsets must start at 0");
+    for (int c = 0; c < n; ++c)
+      if (in.nbr_offsets[c + 1] < in.nbr_offsets[c]) return nfail(DENSE_ERR_INVALID, "CSR offsets decrease");
     for (int c = 0; c < n; ++c)
       for (int k = in.nbr_offsets[c]; k < in.nbr_offsets[c + 1]; ++k)
         if (in.nbr_ids[k] < 0 || in.nbr_ids[k] >= n || (k > in.nbr_offsets[c] && in.nbr_ids[k - 1] >= in.nbr_ids[k]))
@@ -236,6 +236,8 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   const size_t o_list = o;     o = align256(o + sizeof(int) * num_sets);
   if (o > kScratchBytes)
     return nfail(DENSE_ERR_SCRATCH_TOO_SMALL, "batch needs more than the 16 MiB scratch array");
+  // every check above runs on the host; the device is touched from here on
+  if (cudaSetDevice(run->device) != cudaSuccess) return nfail(DENSE_ERR_CUDA, "cudaSetDevice failed");
   unsigned char* base = nullptr;
   int rc = scratch_address(run->device, &base);
   if (rc != DENSE_OK) return rc;

@@ -102,3 +102,32 @@ def test_analysis_checks():
 def test_analysis_range_is_checked_against_the_smallest_set():
     code, text = _code([_set(200, 4), _set(8, 4)], [E.Analysis.basic(["mh1"], 0, 100)])
     assert code == INVALID and "outside the tissue" in text
+
+
+# dense_simulate_noalloc checks its batch on the host before it touches a
+# device, so its refusals need no GPU either.
+SCRATCH_TOO_SMALL = 5
+
+
+def _noalloc_code(sets, precision=E.FP64, analyses=()):
+    import ctypes as C
+    L = E.load("her_model_2014")
+    run, cset, keep = E._describe(L, sets, list(analyses), 0.01, 0.1, precision, 0)
+    f = L.lib.dense_simulate_noalloc
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(E._RunDesc), C.c_int, C.POINTER(E._SetDesc), C.POINTER(C.c_double),
+                  C.POINTER(C.c_int32), C.c_void_p]
+    out = np.zeros(max(1, sum(L.num_species * s.num_cells for s in sets)))
+    return f(C.byref(run), len(sets), cset, out.ctypes.data_as(C.POINTER(C.c_double)), None, None)
+
+
+def test_noalloc_refusals_on_the_host():
+    assert _noalloc_code([_set()] * 65) == SCRATCH_TOO_SMALL                 # more than 64 sets
+    assert _noalloc_code([_set()], precision=E.FP32_KAHAN) == UNSUPPORTED
+    assert _noalloc_code([_set()], analyses=[E.Analysis.basic(["mh1"], 0, 8)]) == UNSUPPORTED
+    assert _noalloc_code([_set(260, 4)]) == INVALID                          # more than 256 cells
+    assert _noalloc_code([_set(duration=-1.0)]) == INVALID
+    assert _noalloc_code([_csr([0, 1, 2], [1, 5])]) == INVALID               # id outside the tissue
+    assert _noalloc_code([_csr([0, 2, 1], [0, 1])]) == INVALID               # offsets decrease
+    assert _noalloc_code([_csr([0, 2, 2], [1, 1])]) == INVALID               # ids not ascending
+    assert _noalloc_code([_set(256, 4, duration=1.0)] * 64) == SCRATCH_TOO_SMALL  # past 16 MiB
