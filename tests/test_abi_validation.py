@@ -131,3 +131,29 @@ def test_noalloc_refusals_on_the_host():
     assert _noalloc_code([_csr([0, 2, 1], [0, 1])]) == INVALID               # offsets decrease
     assert _noalloc_code([_csr([0, 2, 2], [1, 1])]) == INVALID               # ids not ascending
     assert _noalloc_code([_set(256, 4, duration=1.0)] * 64) == SCRATCH_TOO_SMALL  # past 16 MiB
+
+
+def test_every_entry_point_refuses_null_arguments():
+    """NULL engines, graphs and output pointers give DENSE_ERR_INVALID (and
+    destroying NULL is a no-op), before any device call."""
+    lib = E.load("her_model_2014").lib
+    calls = {
+        "dense_engine_run": (None, 1, None), "dense_engine_run_graph": (None, 1, None),
+        "dense_engine_sync": (None,), "dense_engine_reset": (None, None), "dense_engine_status": (None, None),
+        "dense_engine_progress": (None, None, None), "dense_engine_read_state": (None, 0, None),
+        "dense_engine_read_basic": (None, 0, 0, None, None, None, None, None, None, None, None),
+        "dense_engine_read_oscillation": (None, 0, 0, None, None, None, None, None, None),
+        "dense_engine_read_trajectory": (None, 0, 0, None, None, 0, None),
+        "dense_engine_read_oscillation_all": (None, 0, None, None),
+        "dense_engine_copy_trajectory": (None, 0, None, 0, None, None),
+        "dense_engine_trajectory_capacity": (None, 0, None), "dense_engine_info": (None, None, None, None),
+        "dense_engine_ring_info": (None, 0, None, None), "dense_graph_launch": (None, None),
+        "dense_graph_capture": (0, None, None, 0, 0, None), "dense_engine_create": (None, 0, None, None),
+        "dense_engine_plan": (None, 0, None, None, None, None), "dense_model_get_info": (None,),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(*args) == INVALID, name
+        assert lib.dense_last_error(), name
+    assert lib.dense_engine_destroy(None) == 0
+    assert lib.dense_graph_destroy(None) == 0
+    assert lib.dense_model_specie_name(-1) is None and lib.dense_model_reaction_name(10 ** 6) is None
