@@ -444,8 +444,13 @@ int main(int argc, char** argv) {
   // initial concentrations (conc_vector, Sim_Initializer.hpp:138-157)
   std::vector<double> conc;
   std::string conc_path;
+  // (DENSE dereferences a failed reader here and crashes; the file must open)
   if (A.str("d", "initial-conc", &conc_path)) {
     conc = read_reals(conc_path, &csv_ok);
+    if (!csv_ok) {
+      std::cout << "CSV file input failed. CSV file '" << conc_path << "' not found or open.\n";
+      return EXIT_FAILURE;
+    }
     conc.resize(NS, 0.0);
   }
   // -b: one global factor or a per-reaction CSV (history sizing only)
@@ -457,6 +462,10 @@ int main(int argc, char** argv) {
     if (end && *end == 0) pert.assign(NR, v);
     else {
       pert = read_reals(pb, &csv_ok);
+      if (!csv_ok) {
+        std::cout << "CSV file input failed. CSV file '" << pb << "' not found or open.\n";
+        return EXIT_FAILURE;
+      }
       pert.resize(NR, 0.0);
     }
   }
