@@ -36,26 +36,19 @@ def bucket_of(s, levels):
     return (bool(levels > 1), int(math.ceil(math.log2(max(2, s.num_cells)))))
 
 
-def candidates(ordered, cells_log2, default_block):
+def candidates(ordered, cells_log2):
     """Schedules worth timing for a bucket: (schedule, mem_block) pairs.
-    Ordered sets: the wave kernel with every row that fits in shared memory,
-    only the neighbour-read species there, or every row in global memory;
-    others: the register kernel (up to 256 cells) or the memory kernel."""
-    cells = 1 << cells_log2
-    out = []
-    if not ordered and cells <= 256:
-        out.append((E.SCHEDULE_AUTO, 0))
-    for b in MEM_BLOCKS:
-        # a CTA wider than the widest level (ordered) or the set (unordered) idles
-        limit = default_block if ordered else max(32, cells)
-        if b <= limit:
-            out.append((E.SCHEDULE_MEMORY, b))
+    Ordered sets: the wave kernel with the engine's CTA (one thread group
+    per step in flight) or one or two warps (fewer steps in flight, more
+    sets per SM), only the neighbour-read species in shared memory, or
+    every row in global memory; others: the register kernel (up to 256
+    cells) or the memory kernel with a CTA no wider than the set."""
     if ordered:
-        # the wave kernel's CTA is one thread group per step in flight: the
-        # engine's choice, or one or two warps (fewer steps in flight, more
-        # sets per SM)
-        out = [(E.SCHEDULE_MEMORY, 0), (E.SCHEDULE_MEMORY, 32), (E.SCHEDULE_MEMORY, 64),
-               (E.SCHEDULE_SHARED_NEIGHBOUR, 0), (E.SCHEDULE_WAVE_GLOBAL, 0)]
+        return [(E.SCHEDULE_MEMORY, 0), (E.SCHEDULE_MEMORY, 32), (E.SCHEDULE_MEMORY, 64),
+                (E.SCHEDULE_SHARED_NEIGHBOUR, 0), (E.SCHEDULE_WAVE_GLOBAL, 0)]
+    cells = 1 << cells_log2
+    out = [(E.SCHEDULE_AUTO, 0)] if cells <= 256 else []
+    out += [(E.SCHEDULE_MEMORY, b) for b in MEM_BLOCKS if b <= max(32, cells)]
     return out
 
 
@@ -94,12 +87,19 @@ def time_schedule(model, sample, schedule, mem_block, step_size, minutes=1.0, fi
 
 
 class Autotuner:
-    def __init__(self, cache_path=None, sample_sets=8, minutes=1.0, device=0, verbose=False):
+    """`timer(model, sample, schedule, mem_block, step_size, minutes,
+    device=...)` gives a schedule's cell-steps/s (time_schedule by default);
+    `gpu_name` keys the cache (the device's name by default)."""
+
+    def __init__(self, cache_path=None, sample_sets=8, minutes=1.0, device=0, verbose=False, timer=None,
+                 gpu_name=None):
         self.cache_path = cache_path
         self.sample_sets = sample_sets
         self.minutes = minutes
         self.device = device
         self.verbose = verbose
+        self.timer = timer or time_schedule
+        self.gpu_name = gpu_name
         self.cache = {}
         if cache_path and os.path.exists(cache_path):
             with open(cache_path) as f:
@@ -107,13 +107,15 @@ class Autotuner:
         self.log = []
 
     def _key(self, model, bucket):
-        import torch
-        return "%s|%s|%d|%d" % (torch.cuda.get_device_name(self.device), model, bucket[0], bucket[1])
+        if self.gpu_name is None:
+            import torch
+            self.gpu_name = torch.cuda.get_device_name(self.device)
+        return "%s|%s|%d|%d" % (self.gpu_name, model, bucket[0], bucket[1])
 
     def tune(self, model, sets, step_size):
         """Stamp the fastest schedule of each bucket on `sets` (in place);
         returns {bucket: (schedule, mem_block)}."""
-        _, kernel, levels = E.plan(model, sets, step_size, 1.0)
+        _, _, levels = E.plan(model, sets, step_size, 1.0)
         groups = {}
         for i, s in enumerate(sets):
             if s.schedule != E.SCHEDULE_AUTO or s.mem_block:
@@ -128,12 +130,10 @@ class Autotuner:
                 rng = np.random.Generator(np.random.PCG64(len(idx)))
                 pick = rng.choice(idx, size=min(self.sample_sets, len(idx)), replace=False)
                 sample = [sets[i] for i in pick]
-                default_block = int(max(kernel[i] for i in idx)) or 256
                 results = []
-                cands = candidates(bucket[0], bucket[1], default_block)
+                cands = candidates(bucket[0], bucket[1])
                 for cand in cands if len(cands) > 1 else []:
-                    v = time_schedule(model, sample, cand[0], cand[1], step_size, self.minutes,
-                                      device=self.device)
+                    v = self.timer(model, sample, cand[0], cand[1], step_size, self.minutes, device=self.device)
                     results.append((v, cand))
                     self.log.append({"model": model, "bucket": bucket, "schedule": cand, "cell_steps_per_s": v})
                     if self.verbose:
