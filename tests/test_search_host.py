@@ -1,5 +1,6 @@
-"""Host-side facts the surrogate search relies on, checked on the oracle
-(bit-exact with the engine, pinned against DENSE)."""
+"""Host-side parts of the surrogate search: the horizon fact it relies on
+(checked on the oracle, bit-exact with the engine), the parameter encoding,
+synchrony, acceptance and fitness, and the evolution strategy."""
 
 import numpy as np
 
@@ -25,3 +26,73 @@ def test_features_do_not_depend_on_the_horizon_past_the_window():
             res.append(sim.oscillation(0))
         for k in ("amps", "pers", "avg_peak", "ncrit", "samples"):
             assert np.array_equal(np.asarray(res[0][k]), np.asarray(res[1][k]), equal_nan=True), k
+
+
+def test_encode_decode_round_trip():
+    rng = np.random.Generator(np.random.PCG64(3))
+    X = rng.uniform(-1, 1, size=(64, len(S.active_params())))
+    assert np.allclose(S.encode(S.decode(X)), X, atol=1e-6)
+    P = S.draw_candidates(256, 4)
+    E = S.encode(P)
+    assert E.shape == (256, 44) and np.abs(E).max() <= 1.0 + 1e-6
+    # parameters that are zero in the template stay zero
+    zero = np.setdiff1d(np.arange(P.shape[1]), S.active_params())
+    assert (S.decode(X)[:, zero] == 0).all()
+
+
+def test_synchrony_known_answers_on_the_host():
+    t = np.linspace(0, 20, 400)[:, None]
+    assert abs(S.synchrony(np.sin(t) * np.ones((1, 8))) - 1.0) < 1e-12
+    assert abs(S.synchrony(np.concatenate([np.sin(t), -np.sin(t)], 1)) + 1.0) < 1e-12
+    # a constant cell is left out; fewer than two varying cells: undefined
+    with_flat = np.concatenate([np.sin(t), np.sin(t), np.full_like(t, 3.0)], 1)
+    assert abs(S.synchrony(with_flat) - 1.0) < 1e-12
+    assert np.isnan(S.synchrony(np.concatenate([np.sin(t), np.full_like(t, 3.0)], 1)))
+    # quarter-period shift: uncorrelated over whole periods
+    q = np.linspace(0, 2 * np.pi * 10, 4000, endpoint=False)[:, None]
+    assert abs(S.synchrony(np.concatenate([np.sin(q), np.cos(q)], 1))) < 1e-9
+
+
+def test_acceptance_targets_and_fitness():
+    F = {"period": np.array([30.0, 33.0, 33.5, np.nan, 28.0]),
+         "amplitude": np.array([60.0, 50.0, 80.0, 90.0, 10.0]),
+         "synchrony": np.array([0.9, np.nan, 0.1, 0.2, 0.3]),
+         "oscillates": np.array([1.0, 1.0, 1.0, 0.0, 1.0], np.float32)}
+    assert S.accepted(F).tolist() == [True, True, False, False, False]
+    T, M = S.targets(F)
+    assert T.shape == (5, 5) and np.isfinite(T).all()
+    assert M[:, 0].tolist() == [1, 1, 1, 0, 1] and M[1, 2] == 0 and M[:, 4].tolist() == [1] * 5
+    f = S.search_fitness(F)
+    assert f[0] == 0.0 and f[1] == 1.0 and f[3] == 1e3
+    assert abs(f[4] - (2.0 / 3.0 + 0.8)) < 1e-12
+
+
+def _sphere(X):
+    return ((X - 0.3) ** 2).sum(axis=1)
+
+
+def test_sres_converges_on_a_smooth_function():
+    """The evolution strategy alone (no simulator) on a shifted sphere in the
+    search box: steady progress, offspring inside [-1, 1], evaluations
+    counted, the same seed giving the same run."""
+    es = S.SRES(10, _sphere, mu=15, lam=100, seed=4)
+    f0 = float(es.f.min())
+    best = [es.step() for _ in range(200)]
+    # the step sizes adapt through exponential smoothing (alpha 0.2), so
+    # progress is steady rather than fast: ~1.5 -> ~2e-5 here
+    assert best[59] < 0.1 * f0 and best[199] < 0.01 * best[59] and best[199] < 1e-4
+    assert np.abs(es.x).max() <= 1.0 and es.evaluations == 100 * 201
+    es2 = S.SRES(10, _sphere, mu=15, lam=100, seed=4)
+    assert [es2.step() for _ in range(200)] == best
+
+
+def test_sres_gains_from_a_surrogate():
+    """With a surrogate ranking 8x lambda offspring (here an exact one) the
+    strategy reaches a lower fitness for the same number of simulated
+    evaluations."""
+    plain = S.SRES(20, _sphere, mu=15, lam=100, seed=6)
+    screened = S.SRES(20, _sphere, mu=15, lam=100, seed=6, surrogate=lambda X: -_sphere(X), screen=8)
+    for _ in range(25):
+        bp, bs = plain.step(), screened.step()
+    assert plain.evaluations == screened.evaluations
+    assert bs < 0.5 * bp
