@@ -111,7 +111,7 @@ def build_workload(num_sets, minutes, seed):
     return sets, workloads.batch_analyses(200, 0.1)
 
 
-def cpu_sample(kind_pref="reference", num_sets=2, minutes=300.0, seed=7):
+def cpu_sample(kind_pref="reference", num_sets=8, minutes=300.0, seed=7):
     """DENSE (or the oracle port) on the host, one core, a bounded sample:
     `num_sets` sets of the workload for `minutes` simulated minutes."""
     from dense_b200 import workloads
@@ -148,7 +148,7 @@ MIXED_WORKLOAD = ("uneven mixed batch, one captured graph: %d sets, her_model_20
                   "autotuned schedules")
 
 
-def mixed_cpu_sample(groups, minutes=20.0, per_model=2):
+def mixed_cpu_sample(groups, minutes=60.0, per_model=4):
     """DENSE's own CPU path (oracle/_ref) on `per_model` sets of each model
     of the mixed batch, `minutes` each, one host core."""
     from oracle.pyoracle import load_oracle, load_ref
