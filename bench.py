@@ -57,8 +57,9 @@ def peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return d.get("hbm_gbs", 6650.0), "measured"
-    return 6650.0, "fallback"
+        if "hbm_gbs" in d:
+            return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs): frac is of measured"
+    return 6650.0, "fallback 6650 GB/s (no measured peak file): frac is of fallback"
 
 
 def dist_env():
@@ -612,7 +613,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
                          "frac": achieved_gbs / hbm, "traffic": traffic,
                          "basis": "%d algorithmic bytes per cell-step (state read+write, delayed reads); peak "
-                                  "%s (MEASURED_PEAKS.json hbm_gbs)" % (BYTES_PER_CELL_STEP, peak_src),
+                                  "%s" % (BYTES_PER_CELL_STEP, peak_src),
                          "fp64_flops_per_s": FLOPS_PER_CELL_STEP * per_launch_cell_steps / avg_launch_s},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d),
