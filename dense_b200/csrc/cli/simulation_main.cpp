@@ -380,6 +380,22 @@ int main(int argc, char** argv) {
     usage();
     return EXIT_SUCCESS;
   }
+  // DENSE flags outside this command: the stochastic seed (-r) and the
+  // colour switch (-n) change nothing here and are accepted; gradients (-g)
+  // are undefined in DENSE (simulation_width_ is 0 when gradient_index is
+  // taken modulo it, sim/base.cpp:22-31) and analysis of an imported
+  // trajectory (-i, io/csvr_sim.cpp) is not built, so both are refused
+  // rather than ignored
+  if (A.has("g", "gradients")) {
+    std::cout << "Error: [-g | --gradients] is not supported (DENSE's gradient path divides by the tissue width "
+                 "before it is set); give per-cell parameters instead.\n";
+    return EXIT_FAILURE;
+  }
+  if (A.has("i", "data-import")) {
+    std::cout << "Error: [-i | --data-import] (analysis of an imported trajectory) is not supported by this "
+                 "command.\n";
+    return EXIT_FAILURE;
+  }
   dense_model_info mi;
   dense_model_get_info(&mi);
   const int NS = mi.num_species, NP = mi.num_params, NR = mi.num_reactions;

@@ -38,6 +38,8 @@ def _run(cli, args, cwd):
     (["-p", PARAMS, "-c", "10", "-w", "5", "-t", "10", "-s", "0", "-u", "0.1"], "step-size"),
     (["-p", PARAMS, "-t", "10", "-s", "0.01", "-u", "0.1"], "cell-graph"),
     (["-c", "10"], "useless state"),
+    (["-p", PARAMS, "-g", "grad.csv"] + BASE, "--gradients] is not supported"),
+    (["-p", PARAMS, "-i", "data.csv"] + BASE, "--data-import] (analysis of an imported trajectory) is not"),
 ])
 def test_bad_invocations_exit_1_with_a_message(cli, tmp_path, args, msg):
     rc, out = _run(cli, args, tmp_path)
