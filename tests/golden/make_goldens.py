@@ -128,7 +128,26 @@ def run_cli_cases():
                 raise RuntimeError("DENSE failed on %s" % name)
             for f in outs:
                 shutil.copyfile(os.path.join(tmp, f), os.path.join(dst, f))
+                if f in UNDEFINED_ROWS:
+                    _blank_undefined_rows(os.path.join(dst, f), UNDEFINED_ROWS[f])
         print("cli", name, outs)
+
+
+# Rows DENSE prints from past the end of its per-species vectors
+# (BasicAnalysis::show indexes them by species id, measurement/basic.ipp:
+# 69-72; in anlys_basic_b the ids of mh1 and mh13 exceed its three observed
+# species): their numbers change from run to run, so the fixture keeps the
+# species name and marks the values undefined.
+UNDEFINED_ROWS = {"anlys_basic_b.csv": ("mh1,", "mh13,")}
+
+
+def _blank_undefined_rows(path, prefixes):
+    with open(path) as f:
+        lines = f.read().split("\n")
+    lines = [ln.split(",")[0] + ",undefined,undefined,undefined" if ln.startswith(prefixes) else ln
+             for ln in lines]
+    with open(path, "w") as f:
+        f.write("\n".join(lines))
 
 
 def copy_ctest():
