@@ -60,8 +60,20 @@ def _order(scores, indices):
 
 
 def local_top(scores, indices, k):
-    o = _order(np.asarray(scores, np.float64), np.asarray(indices, np.int64))[:k]
-    return np.asarray(scores, np.float64)[o], np.asarray(indices, np.int64)[o]
+    """The k best (score, index) pairs in _order's order.  With k below the
+    count, a partition finds the k-th best score first and only the
+    candidates at or above it (ties included) are sorted."""
+    scores = np.asarray(scores, np.float64)
+    indices = np.asarray(indices, np.int64)
+    n = scores.size
+    if 0 < k < n:
+        s = np.where(np.isnan(scores), -np.inf, scores)
+        kth = np.partition(s, n - k)[n - k]
+        keep = np.nonzero(s >= kth)[0]
+        o = keep[_order(scores[keep], indices[keep])[:k]]
+    else:
+        o = _order(scores, indices)[:max(k, 0)]
+    return scores[o], indices[o]
 
 
 def global_top(scores, indices, k, group=None):

@@ -228,10 +228,12 @@ def screened_search(net, n_candidates, seed, keep=0.01, plain_sample=4096, sim_k
     and is extrapolated per candidate."""
     sim_kwargs = sim_kwargs or {}
     P = draw_candidates(n_candidates, seed)
+    from .distributed import local_top
     t0 = time.perf_counter()
     score = score_candidates(net, P)
+    # the ranking counts the selection of the kept candidates too
+    top = local_top(score, np.arange(n_candidates), max(1, int(round(keep * n_candidates))))[1]
     t_infer = time.perf_counter() - t0
-    top = np.argsort(-score, kind="stable")[:max(1, int(round(keep * n_candidates)))]
     Fs = simulate_features(P[top], log=log, **sim_kwargs)
     acc_s = accepted(Fs)
     # surrogate error on the accepted sets, against their FP64 re-simulation

@@ -69,3 +69,18 @@ def test_two_rank_global_top_and_average():
         top, g0, g1 = res[r]
         assert top == want.tolist()
         assert g0 == [1.5] * 4 and g1 == [15.0] * 6
+
+
+def test_local_top_partition_path_equals_a_full_sort():
+    """local_top's partition prefilter returns exactly the first k of the
+    full order (descending score, ascending index among ties, NaN last)."""
+    from dense_b200.distributed import _order, local_top
+    rng = np.random.Generator(np.random.PCG64(12))
+    for n, k in ((1000, 10), (1000, 999), (1000, 1000), (1000, 1500), (50, 0), (2000, 300)):
+        s = rng.integers(0, 20, size=n).astype(np.float64)   # many ties
+        s[rng.choice(n, size=n // 10, replace=False)] = np.nan
+        idx = rng.permutation(n).astype(np.int64) + 7
+        full = _order(s, idx)[:k]
+        got_s, got_i = local_top(s, idx, k)
+        assert np.array_equal(got_i, idx[full])
+        assert np.array_equal(got_s, s[full], equal_nan=True)
