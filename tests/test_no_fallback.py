@@ -43,3 +43,14 @@ def test_surrogate_fails_loudly_without_a_gpu():
     from dense_b200 import search as S
     with pytest.raises(Exception):
         S.simulate_features(np.tile(S.template(), (2, 1)), cells=8)
+
+
+def test_sharded_simulation_fails_loudly_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from dense_b200 import engine as E, workloads
+    from dense_b200.sharding import simulate_sharded
+    s = workloads.perturbed_set(cells=8, width=4, duration=1.0)
+    with pytest.raises(E.DenseError):
+        simulate_sharded("her_model_2014", [s, s], 0.01, 0.1)
