@@ -98,6 +98,9 @@ def simulate_sharded(model, sets, step_size, analysis_interval, analyses=(), pre
             for j, i in enumerate(mine)]
     parts = [None] * world
     if on:
+        if dist.get_backend(group) == "nccl":
+            import torch
+            torch.cuda.set_device(device)  # NCCL stages the objects on the current device
         dist.all_gather_object(parts, rows, group=group)
     else:
         parts = [rows]
