@@ -289,7 +289,13 @@ bool read_graphml(const std::string& path, Graph* g) {
     std::string b = get("vertex1"), t = get("vertex2");
     if (b.empty()) { b = get("source"); t = get("target"); }
     if (!b.empty() && b[0] == 'n') { b.erase(0, 1); t.erase(0, 1); }
-    long x = std::stol(b), y = std::stol(t);
+    long x = 0, y = 0;
+    try {
+      x = std::stol(b);
+      y = std::stol(t);
+    } catch (const std::exception&) {
+      return false;  // a vertex id that is not a number: the graph is invalid
+    }
     if (x == y) continue;
     verts.insert(x);
     verts.insert(y);

@@ -51,3 +51,15 @@ def test_partial_parameter_set(cli, tmp_path):
     bad.write_text("1,2,3,\n")
     rc, out = _run(cli, ["-p", str(bad)] + BASE, tmp_path)
     assert rc == 1 and "Partial set" in out, out
+
+
+def test_malformed_graph_files(cli, tmp_path):
+    """Graph files whose vertex ids are not numbers, or that hold no edges,
+    are refused like missing ones."""
+    bad = tmp_path / "bad.graphml"
+    bad.write_text('<graphml><graph><edge source="n0" target="nx"/></graph></graphml>\n')
+    empty = tmp_path / "empty.graphml"
+    empty.write_text("<graphml><graph></graph></graphml>\n")
+    for g in (bad, empty):
+        rc, out = _run(cli, ["-p", PARAMS, "-f", str(g), "-t", "10", "-s", "0.01", "-u", "0.1"], tmp_path)
+        assert rc == 1 and "is invalid" in out, out
