@@ -379,7 +379,7 @@ void usage() {
 
 }  // namespace
 
-int main(int argc, char** argv) {
+static int run_cli(int argc, char** argv) {
   Args A;
   A.v.assign(argv + 1, argv + argc);
   if (A.has("h", "help") || A.has("H", "usage") || argc == 1) {
@@ -694,4 +694,16 @@ int main(int argc, char** argv) {
   }
   dense_engine_destroy(eng);
   return EXIT_SUCCESS;
+}
+
+int main(int argc, char** argv) {
+  // a malformed number in an input file (std::stold / std::stol on an
+  // analysis XML value or a graph vertex id) ends the run with a message;
+  // DENSE lets the exception terminate the process
+  try {
+    return run_cli(argc, argv);
+  } catch (const std::exception& e) {
+    std::cout << "Error: malformed input (" << e.what() << ").\n";
+    return EXIT_FAILURE;
+  }
 }

@@ -63,3 +63,12 @@ def test_malformed_graph_files(cli, tmp_path):
     for g in (bad, empty):
         rc, out = _run(cli, ["-p", PARAMS, "-f", str(g), "-t", "10", "-s", "0.01", "-u", "0.1"], tmp_path)
         assert rc == 1 and "is invalid" in out, out
+
+
+def test_malformed_analysis_xml(cli, tmp_path):
+    xml = tmp_path / "a.xml"
+    xml.write_text("<analyses><anlys type=\"basic\"><species>mh1</species><cell-start>zero</cell-start>"
+                   "<cell-end>4</cell-end><time-start>0</time-start><time-end>5</time-end>"
+                   "<out-file>b.csv</out-file></anlys></analyses>")
+    rc, out = _run(cli, ["-p", PARAMS, "-a", str(xml)] + BASE, tmp_path)
+    assert rc == 1 and "malformed input" in out, out
