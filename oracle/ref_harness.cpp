@@ -1,7 +1,7 @@
 // ORACLE PIN -- test infrastructure only.
 //
 // Drives DENSE's own deterministic simulator and analyses (compiled from the
-// DENSE sources where they lie, by oracle/Makefile, into oracle/_ref/)
+// DENSE sources where they lie, by oracle/build.py, into oracle/_ref/)
 // through the same C interface as dense_oracle.cpp, so the tests can check
 // the restatement against the reference itself on identical inputs.
 //
