@@ -157,3 +157,18 @@ def test_every_entry_point_refuses_null_arguments():
     assert lib.dense_engine_destroy(None) == 0
     assert lib.dense_graph_destroy(None) == 0
     assert lib.dense_model_specie_name(-1) is None and lib.dense_model_reaction_name(10 ** 6) is None
+
+
+def test_largest_set_plans_and_one_more_cell_is_refused():
+    """65536 cells is the largest set (16-bit cell ids in the wave kernel's
+    records, and the memory kernel's limit): it plans, in the memory-state
+    kernel; 65537 cells is refused as unsupported."""
+    for model in ("her_model_2014", "turing"):
+        p = workloads.template_params(model)
+        off, ids = default_graph(65536, 256)
+        nbytes, kernel, levels = E.plan(model, [E.ParameterSet(off, ids, p, duration=1.0)], 0.01, 0.1)
+        assert nbytes[0] > 0 and kernel[0] >= 32
+        assert (levels[0] > 1) == (model == "turing")   # Turing reads rows written in the same step
+        off, ids = default_graph(65537, 1)
+        with pytest.raises(E.DenseError, match="error 4"):
+            E.plan(model, [E.ParameterSet(off, ids, p, duration=1.0)], 0.01, 0.1)
