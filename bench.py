@@ -52,6 +52,14 @@ DRAM_BYTES_PER_CELL_STEP = 17.7
 METRIC = "cell-steps/s (FP64 plain)"
 
 
+def batch_workload(num_sets, minutes, with_analyses):
+    """The batched workload's name, the same in both arms' JSON lines."""
+    return ("her_model_2014: %d parameter sets (template x exp(U(ln .5, ln 2)) per set), 200 cells each "
+            "(-c 200 -w 4), dt 0.01 min, %g min, %s"
+            % (num_sets, minutes, "Oscillation(mh1, all cells, window 4 min) every 0.1 min" if with_analyses
+               else "no analyses"))
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -462,9 +470,8 @@ def run_reference(a):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed / a.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "her_model_2014 log-uniform [0.5,2]x sets, 200 cells (-c 200 -w 4), dt 0.01, "
-                                   "Oscillation(mh1) every 0.1 min", "sample_per_step": "%d sets x %g min, one set "
-                                   "per core" % (cores, minutes)},
+            "config": {"workload": batch_workload(a.sets, a.minutes, True),  # the sample runs Oscillation
+                       "sample_per_step": "%d sets x %g min of it, one set per core" % (cores, minutes)},
             "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind,
                              "sample": "%d host processes, each DENSE on one set of 200 cells for %g min per step"
                                        % (cores, minutes)},
@@ -602,10 +609,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": total_ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if precision == E.FP64 else "f32+kahan", "data": "synthetic",
-            "config": {"workload": "her_model_2014: %d parameter sets (template x exp(U(ln .5, ln 2)) per set), "
-                                   "200 cells each (-c 200 -w 4), dt 0.01 min, %g min, %s"
-                                   % (a.sets, a.minutes, "Oscillation(mh1, all cells, window 4 min) every 0.1 min"
-                                      if analyses else "no analyses"),
+            "config": {"workload": batch_workload(a.sets, a.minutes, bool(analyses)),
                        "sets_per_gpu": a.sets, "step": "one launch advancing every set %d chunks (%g min)"
                        % (per_step, per_step * 0.1), "l2": "inputs larger than L2 (history rings + "
                        "windows %.0f MB per GPU)" % (info["device_bytes"] / 1e6),
