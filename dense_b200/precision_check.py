@@ -56,17 +56,12 @@ def compare(num_sets=512, minutes=1200.0, window=float("inf"), seed=2, device=0)
         b.close()
     a, f = out["fp64"], out["fp32"]
     ok = np.isfinite(a["per"]) & np.isfinite(f["per"]) & np.isfinite(a["amp"]) & np.isfinite(f["amp"])
-    rp = np.abs(f["per"][ok] - a["per"][ok]) / np.abs(a["per"][ok])
-    ra = np.abs(f["amp"][ok] - a["amp"][ok]) / np.maximum(np.abs(a["amp"][ok]), 1e-12)
-    fin = np.isfinite(a["state"]) & np.isfinite(f["state"])
-    rs = np.abs(f["state"][fin] - a["state"][fin]) / np.maximum(np.abs(a["state"][fin]), 1e-3)
-
-    def stats(x):
-        return {"median": float(np.median(x)), "p99": float(np.quantile(x, 0.99)), "max": float(np.max(x))} \
-            if x.size else None
-
-    return {"sets": num_sets, "minutes": minutes, "window": window, "sets_compared": int(ok.sum()),
-            "period_rel": stats(rp), "amplitude_rel": stats(ra), "final_state_rel": stats(rs),
+    rp = _rel(f["per"][ok], a["per"][ok], 0.0)
+    ra = _rel(f["amp"][ok], a["amp"][ok], 1e-12)
+    rs = _rel(f["state"], a["state"])
+    return {"config": "batch", "sets": num_sets, "minutes": minutes, "window": window,
+            "sets_compared": int(ok.sum()),
+            "period_rel": _stats(rp), "amplitude_rel": _stats(ra), "final_state_rel": _stats(rs),
             "oscillation_found_mismatch": int((np.isfinite(a["per"]) != np.isfinite(f["per"])).sum()),
             "fp64_cell_steps_per_s": a["cell_steps"] / a["seconds"],
             "fp32_cell_steps_per_s": f["cell_steps"] / f["seconds"]}
