@@ -1,7 +1,8 @@
-"""The schedule autotuner's host logic (dense_b200.autotune) with a fake
-timer in place of GPU timing: buckets, candidate schedules, stamping every
-set of a bucket with its fastest schedule, leaving the caller's own choices
-alone, and the per-GPU cache."""
+"""The uneven mixed batch on the host: the schedule autotuner's logic
+(dense_b200.autotune) with a fake timer in place of GPU timing -- buckets,
+candidate schedules, stamping every set of a bucket with its fastest
+schedule, leaving the caller's own choices alone, the per-GPU cache -- and
+the workload generator (dense_b200.workloads.mixed_sets)."""
 
 import json
 
@@ -74,3 +75,34 @@ def test_tune_stamps_buckets_and_caches(tmp_path):
     t2 = Autotuner(cache_path=cache, sample_sets=2, timer=timer2, gpu_name="fake-gpu")
     assert t2.tune("turing", again["turing"], 0.01) == chosen_turing
     assert timer2.calls == []
+
+
+def test_mixed_workload_matches_its_description():
+    """The uneven mixed batch: her_model_2014 (cells 16..1024 in multiples
+    of 4, width 4, delays U[5, 20] min) or Turing-Pattern (N x N, N in
+    8..64, width N) with probability 1/2, horizons U[100, 1200] min, rates
+    scaled within [1/2, 2]; the same seed gives the same batch."""
+    import numpy as np
+    L = E.load("her_model_2014")
+    d0, d1 = L.num_reactions, L.num_reactions + L.num_delay_reactions
+    g = workloads.mixed_sets(400, seed=3)
+    her, tur = g["her_model_2014"], g["turing"]
+    assert len(her) + len(tur) == 400 and 150 < len(her) < 250
+    hp, tp = workloads.template_params("her_model_2014"), workloads.template_params("turing")
+    for s in her:
+        assert 16 <= s.num_cells <= 1024 and s.num_cells % 4 == 0
+        assert 100.0 <= s.duration <= 1200.0
+        assert ((s.set_params[d0:d1] >= 5.0) & (s.set_params[d0:d1] <= 20.0)).all()
+        nz = hp[:d0] > 0
+        r = s.set_params[:d0][nz] / hp[:d0][nz]
+        assert (r >= 0.5 - 1e-12).all() and (r <= 2.0 + 1e-12).all()
+    for s in tur:
+        n = int(round(np.sqrt(s.num_cells)))
+        assert n * n == s.num_cells and 8 <= n <= 64 and 100.0 <= s.duration <= 1200.0
+        nz = tp > 0
+        r = s.set_params[nz] / tp[nz]
+        assert (r >= 0.5 - 1e-12).all() and (r <= 2.0 + 1e-12).all()
+        assert s.init_conc is not None
+    again = workloads.mixed_sets(400, seed=3)
+    assert [s.num_cells for s in again["turing"]] == [s.num_cells for s in tur]
+    assert all(np.array_equal(a.set_params, b.set_params) for a, b in zip(again["her_model_2014"], her))
