@@ -115,12 +115,26 @@ def _other(model, seed, delay_sets=()):
                           dict(kind="oscillation", species=[0], cells=(0, 24), t=(0.0, INF), win=1.0, intvl=0.1)])
 
 
+def _her_pert_factors():
+    # -b perturbation factors per reaction: they scale the delays that size
+    # DENSE's rings (base.cpp:55-140), so reads at lag S-1 (delays below one
+    # minute truncate to k = 0) see other rows
+    rng = np.random.Generator(np.random.PCG64(5))
+    nsp = len(workloads.templates()["her_model_2014"]["species"])
+    return dict(model="her_model_2014", dt=0.01, interval=0.1,
+                sets=[_set("her_model_2014", 20, 4, 30.0, perturb=rng.uniform(0.0, 0.6, size=34))],
+                analyses=[dict(kind="basic", species=list(range(nsp)), cells=(0, 20), t=(0.0, INF)),
+                          dict(kind="oscillation", species=_her("mh1", "mh13"), cells=(0, 20), t=(0.0, INF),
+                               win=4.0, intvl=0.1)])
+
+
 CASES = {
     "her_test": _her_test,
     "her_pert": _her_pert,
     "her_sets": _her_sets,
     "her_delays": _her_delays,
     "her_init": _her_init,
+    "her_pert_factors": _her_pert_factors,
     "turing": _turing,
     "nan_test": _nan_test,
     "delay_reaction": lambda: _other("delay_reaction", 21, delay_sets=[(100.0, 100.0)]),
