@@ -1192,6 +1192,7 @@ int dense_graph_capture(int num_engines, void* const* run_fns, dense_engine* con
   std::vector<cudaStream_t> st(num_engines, nullptr);
   std::vector<cudaEvent_t> ev(num_engines + 1, nullptr);
   cudaError_t ce = cudaSuccess;
+  int failed = -1;  // the engine whose run failed (its message is in its own library's dense_last_error)
   for (int i = 0; i < num_engines && ce == cudaSuccess; ++i) ce = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
   for (int i = 0; i <= num_engines && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
   int rc = DENSE_OK;
@@ -1202,6 +1203,7 @@ int dense_graph_capture(int num_engines, void* const* run_fns, dense_engine* con
     for (int i = 0; i < num_engines && le == cudaSuccess && rc == DENSE_OK; ++i) {
       le = cudaStreamWaitEvent(st[i], ev[num_engines], 0);
       if (le == cudaSuccess) rc = reinterpret_cast<run_fn>(run_fns[i])(engines[i], num_chunks, st[i]);
+      if (rc != DENSE_OK) failed = i;
       if (le == cudaSuccess && rc == DENSE_OK) le = cudaEventRecord(ev[i], st[i]);
       if (le == cudaSuccess && rc == DENSE_OK) le = cudaStreamWaitEvent(cap, ev[i], 0);
     }
@@ -1216,7 +1218,9 @@ int dense_graph_capture(int num_engines, void* const* run_fns, dense_engine* con
   for (auto x : ev)
     if (x) cudaEventDestroy(x);
   cudaStreamDestroy(cap);
-  if (rc != DENSE_OK) return fail(rc, "capture: " + g_error);
+  if (rc != DENSE_OK)
+    return fail(rc, "capture: the run of engine " + std::to_string(failed) + " failed with code " +
+                        std::to_string(rc) + " (its model library's dense_last_error has the reason)");
   if (ce != cudaSuccess) return fail(DENSE_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
   *graph_exec = ge;
   return DENSE_OK;
