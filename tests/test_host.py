@@ -133,3 +133,33 @@ def test_csv_gen_matches_dense(model, tmp_path):
     assert outs["ours"] == outs["ref"]
     r = subprocess.run([ours], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "Missing required command line argument" in r.stdout
+
+
+def _levels(off, ids):
+    """Dependency levels of DENSE's in-order sweep: a cell comes after every
+    lower-numbered neighbour whose row of this step it reads."""
+    n = len(off) - 1
+    level = [0] * n
+    for c in range(n):
+        lv = [level[v] + 1 for v in ids[off[c]:off[c + 1]] if v < c]
+        level[c] = max(lv) if lv else 0
+    return max(level) + 1
+
+
+def test_plan_levels_of_in_order_reads_on_irregular_tissues():
+    """dense_engine_plan's dependency levels for Turing's in-order neighbour
+    reads, on default grids and random graph-file tissues (0-12
+    neighbours, self-loops), equal an independent count; without in-order
+    reads (her_model_2014) a step is one level."""
+    from dense_b200 import tissue, workloads
+    from dense_b200.engine import ParameterSet, plan
+    from tests.test_oracle import _random_tissue
+    rng = np.random.Generator(np.random.PCG64(77))
+    tp, hp = workloads.template_params("turing"), workloads.template_params()
+    graphs = [tissue.default_graph(N * N, N) for N in (4, 8, 13)]
+    graphs += [_random_tissue(rng, n, 12) for n in (1, 2, 30, 200)]
+    for off, ids in graphs:
+        _, _, lv = plan("turing", [ParameterSet(off, ids, tp, duration=1.0)], 0.01, 0.1)
+        assert lv[0] == _levels(off, ids), (len(off) - 1, lv[0])
+        _, _, lh = plan("her_model_2014", [ParameterSet(off, ids, hp, duration=1.0)], 0.01, 0.1)
+        assert lh[0] == 1
