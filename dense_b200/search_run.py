@@ -35,6 +35,19 @@ import numpy as np
 from . import search as S
 
 
+def with_one_time_cost(res):
+    """The screened search's rate charged with the surrogate's one-time cost
+    (training simulations and training), crediting the sets the training
+    simulations accepted, and its gain over plain search; None where the
+    run has no plain rate."""
+    srch, data = res["search"], res["data"]
+    seconds = data["seconds"] + res["training_s"] + srch["inference_s"] + srch["resimulation_s"]
+    accepted = srch["accepted_screened"] + data["accepted_fraction"] * data["train_sets"]
+    rate = accepted / seconds
+    plain = srch["accepted_per_s_plain"]
+    return {"accepted_per_s": rate, "gain": rate / plain if plain > 0 else None, "seconds": seconds}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=200000)
@@ -69,6 +82,7 @@ def main(argv=None):
     res["held_out_error"] = S.feature_errors(net, P_test, F_test)
     res["search"] = S.screened_search(net, a.candidates, a.seed + 2, keep=a.keep, plain_sample=a.plain_sample,
                                       sim_kwargs=sim, log=log)
+    res["search_with_one_time_cost"] = with_one_time_cost(res)
     if a.generations > 0:
         fit = lambda X: S.search_fitness(S.simulate_features(S.decode(X), **sim))  # noqa: E731
         pred = lambda X: S.predicted_score(net.predict(X.astype(np.float32)))  # noqa: E731

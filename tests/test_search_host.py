@@ -96,3 +96,17 @@ def test_sres_gains_from_a_surrogate():
         bp, bs = plain.step(), screened.step()
     assert plain.evaluations == screened.evaluations
     assert bs < 0.5 * bp
+
+
+def test_gain_with_one_time_cost():
+    """The screened rate charged with training simulations and training,
+    on the figures of a recorded 10M-candidate run (200k training sets)."""
+    from dense_b200.search_run import with_one_time_cost
+    res = {"data": {"seconds": 69.686775528, "train_sets": 200000, "accepted_fraction": 0.03212},
+           "training_s": 49.90117416199999,
+           "search": {"inference_s": 0.4650351440000122, "resimulation_s": 31.993933156999987,
+                      "accepted_screened": 49294, "accepted_per_s_plain": 95.1213437156791}}
+    r = with_one_time_cost(res)
+    assert abs(r["accepted_per_s"] - 366.45) < 0.1 and abs(r["gain"] - 3.85) < 0.01
+    res["search"]["accepted_per_s_plain"] = 0.0
+    assert with_one_time_cost(res)["gain"] is None
