@@ -39,14 +39,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic cost of one her_model_2014 cell-step (FP64):
-#  bytes: the lag-0 state read (14 x 8) and written (14 x 8) plus the
-#         distinct delayed reads (pd, ph11 x3, ph713 x3, md, mh13 and the
-#         neighbour-averaged pd row: 10 x 8) = 304 B;
-#  flops: 34 rates (~89 mul/add/div incl. the two neighbour averages), 52
-#         delta terms (mul + add) and 14 Euler updates (mul + add) = 221.
+# Algorithmic cost of one her_model_2014 cell-step (FP64) at the template
+# parameters, counted by evaluating the model's own rates with a counting
+# arithmetic type (tests/native/count_ops.cpp, checked by
+# tests/test_cost_model.py):
+#  bytes: the lag-0 state read (14 x 8) and written (14 x 8) plus the 10
+#         distinct history rows the rates read (pd at two lags, ph11 and
+#         ph713 at three each, md, mh13) = 304 B;
+#  flops: 34 rates (10 add, 45 mul, 11 div), two neighbour averages (4.5
+#         adds and a division each on the 200-cell width-4 tissue), 52 delta
+#         terms (mul + add) and 14 Euler updates (mul + add) = 209.
 BYTES_PER_CELL_STEP = 304
-FLOPS_PER_CELL_STEP = 221
+FLOPS_PER_CELL_STEP = 209
 DRAM_BYTES_PER_CELL_STEP = 17.7
 
 METRIC = "cell-steps/s (FP64 plain)"
