@@ -338,6 +338,36 @@ def run_turing(a):
     spc = b.info()["total_cell_steps"] // max(1, total_chunks) // sets_n // (N * N)
     done = int(chunks.astype(np.int64).sum()) * spc * N * N
     value = done / (ms / 1e3)
+    status = int((b.status() != 0).sum())
+    b.close()
+    # e2e: the public API from host arrays (create, the whole horizon, every
+    # set's final state back to the host)
+    e2e_s, h2d, d2h, e2e_cells = [], 0, 0, 0
+    for _ in range(max(1, a.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eb = E.Batch("turing", sets, 0.01, 1.0 if a.minutes >= 1.0 else a.minutes, (), device=local)
+        eb.run(-1)
+        states = [eb.state(i) for i in range(len(sets))]
+        eb.sync()
+        e2e_s.append(time.perf_counter() - t0)
+        e2e_cells = eb.info()["total_cell_steps"]
+        eb.close()
+        h2d = sum(x.set_params.nbytes + x.init_conc.nbytes + x.nbr_offsets.nbytes + x.nbr_ids.nbytes for x in sets)
+        d2h = sum(st.nbytes for st in states)
+    cpu = None
+    if not a.no_cpu:
+        from oracle.pyoracle import load_oracle, load_ref
+        lib, kind = load_ref("turing"), "reference"
+        if lib is None:
+            lib, kind = load_oracle("turing"), "port"
+        cpu_minutes = max(1.0, round(2.5e7 / (N * N * 100)))
+        t0 = time.perf_counter()
+        sim = lib.create(off, ids, np.tile(p, (N * N, 1)), p, ic, 0.01)
+        chunks = sim.run(cpu_minutes, 1.0)
+        secs = time.perf_counter() - t0
+        cpu = {"value": chunks * 100 * N * N / secs, "unit": "cell-steps/s", "cores": 1, "kind": kind,
+               "sample": "one set of the grid for %g min on one host core, %.1f s" % (cpu_minutes, secs)}
     hbm, peak_src = peaks()
     achieved = TURING_BYTES_PER_CELL_STEP * value / 1e9
     if rank == 0:
@@ -350,9 +380,12 @@ def run_turing(a):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": None, "basis": "%d algorithmic bytes per Turing cell-step; peak %s"
                                                    % (TURING_BYTES_PER_CELL_STEP, peak_src)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_cells / statistics.median(e2e_s), "unit": "cell-steps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": len(e2e_s),
+                    "what": "Batch() from host arrays + the whole horizon + every set's final state to host"},
             "gpu_launches": a.steps, "clocks": clk,
-            "status_nonzero_sets": int((b.status() != 0).sum())}), flush=True)
-    b.close()
+            "status_nonzero_sets": status}), flush=True)
 
 
 def run_single(a):
