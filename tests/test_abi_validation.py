@@ -172,3 +172,27 @@ def test_largest_set_plans_and_one_more_cell_is_refused():
         off, ids = default_graph(65537, 1)
         with pytest.raises(E.DenseError, match="error 4"):
             E.plan(model, [E.ParameterSet(off, ids, p, duration=1.0)], 0.01, 0.1)
+
+
+def test_perturbation_factors_resize_the_rings():
+    """-b factors scale the delays that size DENSE's rings (S = (int)(max
+    delay x (1 + factor) / dt) + 2).  mh13 is read at delay 0.805 min
+    (k = 0, so lag S - 1): a factor of 0.6 on ph13_synthesis takes its S
+    from 82 to 130 rows (as in DENSE, checked on the oracle), which doubles
+    the register kernel's power-of-two staging of mh13 from 128 to 256
+    rows; the plan grows by exactly those rows."""
+    from oracle.pyoracle import load_oracle
+    L = E.load("her_model_2014")
+    p = workloads.template_params()
+    off, ids = default_graph(20, 4)
+    pert = np.zeros(L.num_reactions)
+    pert[L.reactions.index("ph13_synthesis")] = 0.6
+    mh13 = L.species.index("mh13")
+    O = load_oracle("her_model_2014")
+    S0 = O.create(off, ids, np.tile(p, (20, 1)), p, None, 0.01).ring_sizes()[0]
+    S1 = O.create(off, ids, np.tile(p, (20, 1)), p, None, 0.01, pert).ring_sizes()[0]
+    assert S0[mh13] == 82 and S1[mh13] == 130
+    assert [S0[i] for i in range(14) if i != mh13] == [S1[i] for i in range(14) if i != mh13]
+    b0, _, _ = E.plan("her_model_2014", [E.ParameterSet(off, ids, p, duration=1.0)], 0.01, 0.1)
+    b1, _, _ = E.plan("her_model_2014", [E.ParameterSet(off, ids, p, duration=1.0, perturb=pert)], 0.01, 0.1)
+    assert b1[0] - b0[0] == 8 * (256 - 128) * 20

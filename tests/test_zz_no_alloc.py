@@ -5,8 +5,8 @@ loop that must not call cudaMalloc after start-up).
 Called through the C ABI twice in a row on the same batch; both results
 must equal, bit for bit (the FP64 tolerance of every other test here), the
 final state the allocating entry points (dense_engine_create / run /
-read_state) give.  This file is collected last, so a failure here comes
-after every other test has run.
+read_state) give.  This file is collected after the engine, CLI, mixed and
+surrogate tests, so a failure here comes after all of them have run.
 """
 
 import ctypes as C
