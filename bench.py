@@ -22,6 +22,13 @@ exchange; scaling is weak); times are the max over ranks.
 --impl reference: DENSE's own deterministic path (compiled from its sources
 into oracle/_ref by oracle/build.py) on every host core, each step a bounded
 sample of the same workload.
+
+Other workloads (--workload; each prints the same JSON keys):
+  single  one her_model_2014 set of 200 cells, every parameter of every cell
+          x U(0.95, 1.05), 600 min, Basic + Oscillation (a step = the run);
+  mixed   10,000 her_model_2014 and Turing-Pattern sets of uneven size and
+          horizon in one captured graph, autotuned schedules;
+  turing  sets of one Turing-Pattern N x N grid (--grid), the wave kernel.
 """
 
 import argparse
