@@ -517,7 +517,8 @@ int oracle_add_conccheck(void* h, int target, int cmin, int cmax, double lo, dou
   return static_cast<int>(s->order.size() - 1);
 }
 
-// Raw Euler steps, no analyses (Deterministic_Simulation::step).
+// Raw Euler steps, no analyses (Deterministic_Simulation::step,
+// sim/determ/determ.cpp:77-88).
 void oracle_steps(void* h, long n) {
   Sim* s = static_cast<Sim*>(h);
   for (long i = 0; i < n; ++i) step(*s);
