@@ -8,9 +8,9 @@ Each library is compiled for sm_100a only, in-tree, into
 * ``kernels_fp32.cu`` (FP32 rates, Kahan-compensated state);
 * ``engine_api.cu``, the host set-up and the C ABI of include/dense_b200.h.
 
-The model headers come from the model directory (dense_b200.models).
-When that directory is absent but a library was built before, the prebuilt
-library is used as is.
+The model headers come from the model directory inside the DENSE tree
+named by $DENSE_REF_DIR (dense_b200.models).  When the variable is unset
+but a library was built before, the prebuilt library is used as is.
 """
 
 import concurrent.futures as cf
@@ -67,8 +67,8 @@ def _run(cmd):
 
 def build_model(model, force=False, verbose=False):
     out = lib_path(model)
-    mdir = model_dir(model)
-    if not os.path.isdir(mdir):
+    mdir = model_dir(model, required=not os.path.exists(out))
+    if mdir is None or not os.path.isdir(mdir):
         if os.path.exists(out):
             return out
         raise RuntimeError("DENSE model directory %s not found and no prebuilt %s" % (mdir, out))

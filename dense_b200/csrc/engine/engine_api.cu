@@ -34,6 +34,7 @@
 #include "dense_b200.h"
 #include "engine_launch.hpp"
 #include "engine_types.hpp"
+#include "lag_trace.hpp"
 
 using namespace dense_b200;
 
@@ -60,59 +61,6 @@ struct NvtxRange {
   ~NvtxRange() { nvtxRangePop(); }
   NvtxRange(const NvtxRange&) = delete;
   NvtxRange& operator=(const NvtxRange&) = delete;
-};
-
-// Dependency tracer (the DummyContext of sim/base.cpp:62-95).
-struct DepContext {
-  bool* deps;
-  double getCon(specie_id sp, int = 0) const { deps[sp] = true; return 0.0; }
-  double calculateNeighborAvg(specie_id sp, int = 0) const { deps[sp] = true; return 0.0; }
-  double getRate(reaction_id) const { return 0.0; }
-  double getDelay(delay_reaction_id) const { return 0.0; }
-  double getCritVal(critspecie_id) const { return 0.0; }
-};
-
-// Records, for one cell, the lag of every history read its reactions make,
-// using the same lag arithmetic as the device context.  Concentrations are
-// stand-ins; several passes with different stand-ins reach reads behind
-// data-dependent branches.  A read missed here is still caught on the
-// device (DENSE_SET_UNSTAGED_LAG).
-struct LagTracer {
-  const double* prm;
-  const double* conc;
-  double nbr_value;
-  const int* S;
-  int* own_max;   // [NS] deepest own lag
-  int* nbr_max;   // [NS] deepest neighbour lag, -1 none
-  bool* ordered;  // a neighbour read of lag S-1
-  bool* bad;
-  bool* ord_sp;   // [NS] species read by neighbours at lag S-1
-  int* plain_min; // [NS] shallowest other neighbour lag (INT_MAX none)
-  int* plain_max; // [NS] deepest other neighbour lag (-1 none)
-  double getCon(specie_id sp) const { return conc[sp]; }
-  double getCon(specie_id sp, int k) const {
-    const int s = S[sp];
-    if (k < 0 || k > s + 1) *bad = true;
-    const int lag = (((k - 1) % s) + s) % s;
-    own_max[sp] = std::max(own_max[sp], lag);
-    return conc[sp];
-  }
-  double calculateNeighborAvg(specie_id sp, int k = 0) const {
-    const int s = S[sp];
-    if (k < 0 || k > s) *bad = true;
-    const int lag = ((k % s) + s) % s;
-    if (lag == s - 1 && s > 1) {
-      *ordered = ord_sp[sp] = true;
-    } else {
-      plain_min[sp] = std::min(plain_min[sp], lag);
-      plain_max[sp] = std::max(plain_max[sp], lag);
-    }
-    nbr_max[sp] = std::max(nbr_max[sp], lag);
-    return nbr_value;
-  }
-  double getRate(reaction_id r) const { return prm[r]; }
-  double getDelay(delay_reaction_id d) const { return prm[NUM_REACTIONS + d]; }
-  double getCritVal(critspecie_id c) const { return prm[NUM_REACTIONS + NUM_DELAY_REACTIONS + c]; }
 };
 
 struct SetPlan {
@@ -324,28 +272,8 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
   const int n = in.num_cells;
   SetDesc& d = plan.d;
   d.n_cells = n;
-  // max_delays (base.cpp:55-140); the gradient loop there never runs
-  // (circumference_ is 0 at that point), so max_gradient is 1.
-  bool deps[NUM_REACTIONS][NUM_SPECIES] = {};
-#define REACTION(name) { DepContext c{deps[name]}; reaction<name>::active_rate(c); }
-#include "reactions_list.hpp"
-#undef REACTION
-  double max_delays[NUM_SPECIES] = {};
-  for (int dr = 0; dr < NUM_DELAY_REACTIONS; ++dr) {
-    const int r = dense_delay_reaction_of[dr];
-    const double pert = in.perturb ? in.perturb[r] : 0.0;
-    for (int sp = 0; sp < NUM_SPECIES; ++sp) {
-      if (!deps[r][sp]) continue;
-      const double v = in.set_params[NUM_REACTIONS + dr] * 1.0 * (1.0 + pert);
-      max_delays[sp] = (v < max_delays[sp]) ? max_delays[sp] : v;
-    }
-  }
-  for (int sp = 0; sp < NUM_SPECIES; ++sp) {
-    const double v = max_delays[sp] / dt + 2;  // baby_cl.cpp:10
-    if (!(v >= 1.0 && v < 2147483647.0))
-      return fail(DENSE_ERR_INVALID, "ring size of species " + std::to_string(sp) + " is not a positive int");
-    d.S[sp] = static_cast<int>(v);
-  }
+  // DENSE's ring sizes (base.cpp:55-140, baby_cl.cpp:10)
+  if (!ring_sizes(in, dt, d.S)) return fail(DENSE_ERR_INVALID, "a ring size is not a positive int");
   // parameters for the device: one row [NP] when every cell uses the set's
   // parameters, else [NP][n]; NaN rates/delays reject the set, as DENSE's
   // getRate/getDelay throw (sim/base.hpp:398-412)
@@ -359,31 +287,16 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
       if (i < NUM_REACTIONS + NUM_DELAY_REACTIONS && std::isnan(p[i])) plan.status |= kSetNanParam;
     }
   }
-  // traced lags
-  int own_max[NUM_SPECIES], nbr_max[NUM_SPECIES];
-  for (int sp = 0; sp < NUM_SPECIES; ++sp) { own_max[sp] = 0; nbr_max[sp] = -1; }
-  bool ordered = false, bad = false;
-  bool ord_sp[NUM_SPECIES] = {};
-  int plain_min[NUM_SPECIES], plain_max[NUM_SPECIES];
-  for (int sp = 0; sp < NUM_SPECIES; ++sp) {
-    plain_min[sp] = std::numeric_limits<int>::max();
-    plain_max[sp] = -1;
-  }
-  double prm[NUM_PARAMS];
-  double conc[NUM_SPECIES];
-  const double nbr_values[4] = {0.0, 2.0, 0.5, 7.25};
-  // cells sharing the set's parameters all read the same lags: trace one
-  const int traced = in.cell_params ? n : 1;
-  for (int c = 0; c < traced; ++c) {
-    for (int i = 0; i < NUM_PARAMS; ++i) prm[i] = cell_params[static_cast<size_t>(i) * pcols + c];
-    for (int pass = 0; pass < 4; ++pass) {
-      for (int sp = 0; sp < NUM_SPECIES; ++sp) conc[sp] = pass == 0 ? 0.0 : (pass == 1 ? 1.0 : 0.37 * (sp + pass));
-      LagTracer t{prm, conc, nbr_values[pass], d.S, own_max, nbr_max, &ordered, &bad, ord_sp, plain_min, plain_max};
-#define REACTION(name) reaction<name>::active_rate(t);
-#include "reactions_list.hpp"
-#undef REACTION
-    }
-  }
+  // traced lags; cells sharing the set's parameters all read the same
+  // lags, so one is traced
+  LagTrace tr;
+  trace_lags(cell_params.data(), in.cell_params ? n : 1, 1, pcols, d.S, tr);
+  const int* own_max = tr.own_max;
+  const int* nbr_max = tr.nbr_max;
+  const bool* ord_sp = tr.ord_sp;
+  const int* plain_min = tr.plain_min;
+  const int* plain_max = tr.plain_max;
+  const bool ordered = tr.ordered, bad = tr.bad;
   if (bad) plan.status |= kSetBadDelay;
   // sets whose neighbour reads see the row written in the same step, and
   // sets larger than a CTA, run in the memory-state kernel, which keeps

@@ -15,10 +15,20 @@
 // The array is a file-scope __device__ variable of kScratchBytes (16 MiB);
 // every GPU that loads this library keeps it until the process exits.  In
 // host code the name g_noalloc_scratch is only a stand-in for the device
-// symbol, never a usable address, so the first call on each device (with
-// that device current) asks the runtime for the real address with
-// cudaGetSymbolAddress and keeps it.  That first call should therefore come
-// before any stream capture on the device.
+// symbol, never a usable address, so every call (with the run's device
+// current) asks the runtime for the real address with cudaGetSymbolAddress,
+// which allocates nothing; asking on every call rather than caching keeps
+// the address right if the device's context is ever re-created.  The first
+// call on a device may load this library's device code there, so it should
+// come before any stream capture on the device.
+//
+// The call makes run->device current while it works and makes the caller's
+// current device current again before it returns.
+//
+// It runs sets in the register kernel only.  A set whose neighbour reads
+// see the row written in the same step (DENSE's in-order cell loop, as in
+// Turing-Pattern) needs the memory or wave kernel and is refused with
+// DENSE_ERR_UNSUPPORTED before the device is touched.
 //
 // All calls share the one array and it keeps the previous call's contents.
 // Everything the kernels read is written by the call itself before the
@@ -33,7 +43,6 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "dense_model_api.hpp"
@@ -43,71 +52,41 @@
 #include "dense_b200.h"
 #include "engine_launch.hpp"
 #include "engine_types.hpp"
+#include "lag_trace.hpp"
 
 using namespace dense_b200;
 
 namespace {
 
 constexpr size_t kScratchBytes = size_t(16) << 20;
-constexpr int kMaxDevices = 64;
 constexpr int kMaxNoallocSets = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
-
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
 
 // Failures are reported by return code only (the message names the case
 // for readers of this file).
 int nfail(int code, const char*) { return code; }
 
-// Device address of the scratch array on the current device (set-up on
-// first use per device).
-int scratch_address(int device, unsigned char** out) {
-  if (device < 0 || device >= kMaxDevices) return nfail(DENSE_ERR_INVALID, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return nfail(DENSE_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
-    g_scratch_ptr[device] = p;
-  }
-  *out = static_cast<unsigned char*>(g_scratch_ptr[device]);
+// Device address of the scratch array on the current device.
+int scratch_address(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) return nfail(DENSE_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+  *out = static_cast<unsigned char*>(p);
   return DENSE_OK;
 }
 
-struct Dep {
-  bool* deps;
-  double getCon(specie_id sp, int = 0) const { deps[sp] = true; return 0.0; }
-  double calculateNeighborAvg(specie_id sp, int = 0) const { deps[sp] = true; return 0.0; }
-  double getRate(reaction_id) const { return 0.0; }
-  double getDelay(delay_reaction_id) const { return 0.0; }
-  double getCritVal(critspecie_id) const { return 0.0; }
-};
-
-struct Lags {
-  const double* prm;
-  const int* S;
-  int* own_max;
-  int* nbr_max;
-  bool* ordered;
-  double getCon(specie_id) const { return 0.0; }
-  double getCon(specie_id sp, int k) const {
-    const int s = S[sp];
-    const int lag = (((k - 1) % s) + s) % s;
-    if (lag > own_max[sp]) own_max[sp] = lag;
-    return 0.0;
+// Makes the caller's current device current again when the call returns.
+struct DeviceRestore {
+  int prev = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
   }
-  double calculateNeighborAvg(specie_id sp, int k = 0) const {
-    const int s = S[sp];
-    const int lag = ((k % s) + s) % s;
-    if (lag == s - 1 && s > 1) *ordered = true;
-    if (lag > nbr_max[sp]) nbr_max[sp] = lag;
-    return 0.0;
+  ~DeviceRestore() {
+    if (prev >= 0) cudaSetDevice(prev);
   }
-  double getRate(reaction_id r) const { return prm[r]; }
-  double getDelay(delay_reaction_id d) const { return prm[NUM_REACTIONS + d]; }
-  double getCritVal(critspecie_id c) const { return prm[NUM_REACTIONS + NUM_DELAY_REACTIONS + c]; }
+  DeviceRestore(const DeviceRestore&) = delete;
+  DeviceRestore& operator=(const DeviceRestore&) = delete;
 };
 
 // Writes the [NP][n] parameter layout of one set from its raw rows.
@@ -158,39 +137,22 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
     SetDesc& d = desc[si];
     std::memset(&d, 0, sizeof(d));
     d.n_cells = n;
-    bool deps[NUM_REACTIONS][NUM_SPECIES] = {};
-#define REACTION(name) { Dep c{deps[name]}; reaction<name>::active_rate(c); }
-#include "reactions_list.hpp"
-#undef REACTION
-    double md[NUM_SPECIES] = {};
-    for (int dr = 0; dr < NUM_DELAY_REACTIONS; ++dr) {
-      const int r = dense_delay_reaction_of[dr];
-      const double pert = in.perturb ? in.perturb[r] : 0.0;
-      for (int sp = 0; sp < NUM_SPECIES; ++sp)
-        if (deps[r][sp]) {
-          const double v = in.set_params[NUM_REACTIONS + dr] * 1.0 * (1.0 + pert);
-          md[sp] = (v < md[sp]) ? md[sp] : v;
-        }
-    }
-    for (int sp = 0; sp < NUM_SPECIES; ++sp) {
-      const double v = md[sp] / dt + 2;
-      if (!(v >= 1.0 && v < 2147483647.0)) return nfail(DENSE_ERR_INVALID, "ring size is not a positive int");
-      d.S[sp] = static_cast<int>(v);
-    }
-    int own_max[NUM_SPECIES], nbr_max[NUM_SPECIES];
-    for (int sp = 0; sp < NUM_SPECIES; ++sp) { own_max[sp] = 0; nbr_max[sp] = -1; }
-    bool ordered = false;
+    if (!ring_sizes(in, dt, d.S)) return nfail(DENSE_ERR_INVALID, "ring size is not a positive int");
     int status0 = 0;
-    for (int c = 0; c < (in.cell_params ? n : 1); ++c) {
-      const double* prm = in.cell_params ? in.cell_params + static_cast<size_t>(c) * NUM_PARAMS : in.set_params;
+    const int traced = in.cell_params ? n : 1;
+    const double* prm0 = in.cell_params ? in.cell_params : in.set_params;
+    for (int c = 0; c < traced; ++c)
       for (int i = 0; i < NUM_REACTIONS + NUM_DELAY_REACTIONS; ++i)
-        if (std::isnan(prm[i])) status0 |= kSetNanParam;
-      Lags t{prm, d.S, own_max, nbr_max, &ordered};
-#define REACTION(name) reaction<name>::active_rate(t);
-#include "reactions_list.hpp"
-#undef REACTION
-    }
-    if (ordered) status0 |= kSetOrderedReads;
+        if (std::isnan(prm0[static_cast<size_t>(c) * NUM_PARAMS + i])) status0 |= kSetNanParam;
+    // the same tracing as dense_engine_create, so the rings have the same depths
+    LagTrace tr;
+    trace_lags(prm0, traced, NUM_PARAMS, 1, d.S, tr);
+    if (tr.ordered)
+      return nfail(DENSE_ERR_UNSUPPORTED,
+                   "neighbour reads of the row written in the same step need the memory or wave kernel");
+    if (tr.bad) status0 |= kSetBadDelay;
+    const int* own_max = tr.own_max;
+    const int* nbr_max = tr.nbr_max;
     int64_t off = 0;
     for (int sp = 0; sp < NUM_SPECIES; ++sp) {
       int depth = 0;
@@ -237,9 +199,10 @@ extern "C" DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int n
   if (o > kScratchBytes)
     return nfail(DENSE_ERR_SCRATCH_TOO_SMALL, "batch needs more than the 16 MiB scratch array");
   // every check above runs on the host; the device is touched from here on
+  DeviceRestore restore_;
   if (cudaSetDevice(run->device) != cudaSuccess) return nfail(DENSE_ERR_CUDA, "cudaSetDevice failed");
   unsigned char* base = nullptr;
-  int rc = scratch_address(run->device, &base);
+  int rc = scratch_address(&base);
   if (rc != DENSE_OK) return rc;
 
 #define NA_TRY(x) do { if ((x) != cudaSuccess) return nfail(DENSE_ERR_CUDA, #x " failed"); } while (0)

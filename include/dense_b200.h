@@ -269,13 +269,19 @@ DENSE_API int dense_engine_plan(const dense_run_desc* run, int num_sets, const d
    of at most 256 cells, and the batch's descriptors, parameters, neighbour
    lists, state and history rings must fit in 16 MiB; a larger batch returns
    DENSE_ERR_SCRATCH_TOO_SMALL.  precision must be DENSE_FP64 and
-   num_analyses 0 (DENSE_ERR_UNSUPPORTED otherwise).
-   The first call on a device looks up the array's device address (with that
-   device current); make that first call before any stream capture on the
-   device.  All calls share the array: calls that overlap on the GPU (two
-   host threads, or two streams not ordered against each other) race and
-   must not be made.  Every region a call reads is written by the same call
-   first, so the array's previous contents never leak into results. */
+   num_analyses 0, and no set may have neighbour reads of the row written in
+   the same step (DENSE's in-order cell loop, e.g. Turing-Pattern): those
+   need the memory or wave kernel of dense_engine_create, and such a batch
+   returns DENSE_ERR_UNSUPPORTED before the device is touched.
+   Every call looks up the array's device address on run->device (a lookup
+   that allocates nothing); the first call on a device may load this
+   library's device code there, so make it before any stream capture on the
+   device.  The call makes run->device current while it works and restores
+   the caller's current device before it returns.  All calls share the
+   array: calls that overlap on the GPU (two host threads, or two streams
+   not ordered against each other) race and must not be made.  Every region
+   a call reads is written by the same call first, so the array's previous
+   contents never leak into results. */
 DENSE_API int dense_simulate_noalloc(const dense_run_desc* run, int num_sets, const dense_set_desc* sets,
                                      double* final_state, int32_t* status, void* stream);
 

@@ -15,9 +15,10 @@ Three kinds of artefact, per DENSE model:
   output; ``oracle/_ref/<model>_csv_gen`` -- DENSE's ``csv_gen`` (the
   parameter-file templates), for the same check of ours.
 
-The DENSE tree is ``$DENSE_REF_DIR`` (default /root/reference).  When it
-is absent (a machine that only runs the prebuilt libraries) the reference
-builds are skipped.  Flags follow what DENSE needs to build with g++ 13:
+The DENSE tree is ``$DENSE_REF_DIR``; ``use_default_tree`` points it at
+the checkout this recipe was written for when the variable is unset and
+that checkout exists.  When no tree is named (a machine that only runs the
+prebuilt libraries) the reference builds are skipped.  Flags follow what DENSE needs to build with g++ 13:
 ``-include array -include fstream -include cstdint`` for headers it forgot,
 ``-DNDEBUG`` because the assert at sim/determ/determ.cpp:10 names an
 undeclared variable, and ezxml compiled as C.
@@ -63,6 +64,16 @@ REF_FLAGS = ["-O3", "-DNDEBUG", "-std=c++14", "-w",
              "-include", "array", "-include", "fstream", "-include", "cstdint"]
 
 
+# the DENSE checkout this recipe reads when $DENSE_REF_DIR is unset
+DEFAULT_TREE = "/root/reference"
+
+
+def use_default_tree():
+    """Set $DENSE_REF_DIR to DEFAULT_TREE when unset and that tree exists."""
+    if not os.environ.get("DENSE_REF_DIR") and os.path.isdir(DEFAULT_TREE):
+        os.environ["DENSE_REF_DIR"] = DEFAULT_TREE
+
+
 def _run(cmd):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -99,10 +110,10 @@ REF_CSV_GEN = ["csv_gen.cpp", "io/csvw.cpp", "io/csvr.cpp", "utility/color.cpp",
 def build_oracle(model, force=False):
     """Compile the restatement for one model (needs the model headers)."""
     out = oracle_lib_path(model)
-    mdir = model_dir(model)
+    mdir = model_dir(model, required=not os.path.exists(out))
     src = os.path.join(HERE, "dense_oracle.cpp")
     hdr = os.path.join(API_DIR, "dense_model_api.hpp")
-    if not os.path.isdir(mdir):
+    if mdir is None or not os.path.isdir(mdir):
         if os.path.exists(out):
             return out
         raise RuntimeError("model directory %s not found and no prebuilt %s" % (mdir, out))
@@ -124,7 +135,10 @@ def _ezxml_obj():
 
 def build_ref(model, force=False, cli=True):
     """Compile DENSE's own deterministic path for one model, if present."""
-    srcdir = os.path.join(dense_dir(), "source")
+    tree = dense_dir(required=False)
+    if tree is None:
+        return None
+    srcdir = os.path.join(tree, "source")
     mdir = model_dir(model)
     if not os.path.isdir(srcdir) or not os.path.isdir(mdir):
         return None
@@ -156,5 +170,6 @@ def build_all(models=None, force=False):
 
 
 if __name__ == "__main__":
+    use_default_tree()
     for m, (o, r) in build_all(sys.argv[1:] or None, force=True).items():
         print(m, o, r)

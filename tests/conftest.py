@@ -9,6 +9,9 @@ if ROOT not in sys.path:
 
 
 def pytest_configure(config):
+    # the DENSE tree the fixtures and model builds read, when one is present
+    from oracle.build import use_default_tree
+    use_default_tree()
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
 
 

@@ -27,6 +27,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from oracle.build import use_default_tree  # noqa: E402
+
+use_default_tree()
+
 from dense_b200.models import dense_dir  # noqa: E402
 from tests.golden.cases import CASES, build_case  # noqa: E402
 

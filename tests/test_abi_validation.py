@@ -109,9 +109,9 @@ def test_analysis_range_is_checked_against_the_smallest_set():
 SCRATCH_TOO_SMALL = 5
 
 
-def _noalloc_code(sets, precision=E.FP64, analyses=()):
+def _noalloc_code(sets, precision=E.FP64, analyses=(), model="her_model_2014"):
     import ctypes as C
-    L = E.load("her_model_2014")
+    L = E.load(model)
     run, cset, keep = E._describe(L, sets, list(analyses), 0.01, 0.1, precision, 0)
     f = L.lib.dense_simulate_noalloc
     f.restype = C.c_int
@@ -131,6 +131,20 @@ def test_noalloc_refusals_on_the_host():
     assert _noalloc_code([_csr([0, 2, 1], [0, 1])]) == INVALID               # offsets decrease
     assert _noalloc_code([_csr([0, 2, 2], [1, 1])]) == INVALID               # ids not ascending
     assert _noalloc_code([_set(256, 4, duration=1.0)] * 64) == SCRATCH_TOO_SMALL  # past 16 MiB
+
+
+def test_noalloc_refuses_in_order_neighbour_reads_on_the_host():
+    """A Turing-Pattern set reads its neighbours' rows of the same step
+    (DENSE's in-order cell loop): the register kernel, the only kernel the
+    no-allocation entry point runs, cannot run it, so the call is refused
+    instead of returning an unsimulated state."""
+    off, ids = default_graph(16, 4)
+    p = workloads.template_params("turing")
+    ic = np.array(workloads.templates()["turing"]["init_conc"])
+    ordered = E.ParameterSet(off, ids, p, init_conc=ic, duration=1.0)
+    assert _noalloc_code([ordered], model="turing") == UNSUPPORTED
+    # and so is a batch where only one of several sets is ordered
+    assert _noalloc_code([ordered] * 3, model="turing") == UNSUPPORTED
 
 
 def test_every_entry_point_refuses_null_arguments():

@@ -51,8 +51,8 @@ def test_oracle_is_clean_under_asan_and_ubsan(tmp_path):
         model = build_case(name)["model"]
         if model in libs:
             continue
-        mdir = model_dir(model)
-        if not os.path.isdir(mdir):
+        mdir = model_dir(model, required=False)
+        if mdir is None or not os.path.isdir(mdir):
             pytest.skip("DENSE model headers not present")
         out = str(tmp_path / ("liboracle_%s_san.so" % model))
         r = subprocess.run(["g++", "-O1", "-g", "-std=c++17", "-fPIC", "-shared", "-w", "-fno-omit-frame-pointer",

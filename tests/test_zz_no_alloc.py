@@ -2,10 +2,12 @@
 allocate device memory (a framework that owns the GPU's memory pool, or a
 loop that must not call cudaMalloc after start-up).
 
-Called through the C ABI twice in a row on the same batch; both results
-must equal, bit for bit (the FP64 tolerance of every other test here), the
-final state the allocating entry points (dense_engine_create / run /
-read_state) give.  This file is collected after the engine, CLI, mixed and
+Called through the C ABI twice in a row on the same batch (sets with one
+parameter row, sets with per-cell parameter matrices, and a set with a NaN
+rate that DENSE would reject); both results must equal, bit for bit (the
+FP64 tolerance of every other test here), the final state and the status
+words the allocating entry points (dense_engine_create / run / read_state /
+status) give.  This file is collected after the engine, CLI, mixed and
 surrogate tests, so a failure here comes after all of them have run.
 """
 
@@ -25,8 +27,14 @@ def _inputs():
     P = workloads.log_uniform_params(5, seed=21)
     off, ids = default_graph(48, 4)
     sets = [E.ParameterSet(off, ids, P[i], duration=20.0) for i in range(5)]
-    pert = workloads.perturbed_set(cells=40, width=5, duration=15.0, seed=22)
-    sets.append(pert)
+    # two sets with per-cell parameter matrices, one after the other (each
+    # goes through the shared staging area into the [param][cell] layout)
+    sets.append(workloads.perturbed_set(cells=40, width=5, duration=15.0, seed=22))
+    sets.append(workloads.perturbed_set(cells=24, width=4, duration=12.0, seed=23))
+    # a set DENSE would reject (a NaN rate): its status word must say so
+    bad = P[0].copy()
+    bad[3] = np.nan
+    sets.append(E.ParameterSet(off, ids, bad, duration=5.0))
     return sets
 
 
@@ -64,13 +72,14 @@ def test_noalloc_matches_allocating_entry_point_twice():
     b.run()
     b.sync()
     want = np.concatenate([b.state(i).ravel() for i in range(len(sets))])
-    assert (b.status() == 0).all()
+    want_status = b.status()
+    assert (want_status[:-1] == 0).all() and want_status[-1] == 2  # DENSE_SET_NAN_PARAM
     b.close()
     run = E._RunDesc(E.FP64, 0.01, 0.1, 0, None, 0)
     for _ in range(2):
         rc, got, status = _noalloc(L, sets, run)
         assert rc == 0
-        assert (status == 0).all()
+        assert np.array_equal(status, want_status)
         assert np.array_equal(got, want)
 
 
