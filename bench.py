@@ -131,6 +131,34 @@ def build_workload(num_sets, minutes, seed):
     return sets, workloads.batch_analyses(200, 0.1)
 
 
+PARITY_FIXTURE = os.path.join("tests", "golden", "ref_her_cfg2_full.npz")
+
+
+def batch_parity(batch):
+    """The timed run's own results for the workload's sets that DENSE itself
+    simulated into PARITY_FIXTURE (same seeds, 200 cells, 1200 min,
+    Oscillation of mh1): final state and oscillation outputs, bit for bit."""
+    path = os.path.join(ROOT, PARITY_FIXTURE)
+    if not os.path.exists(path):
+        return {"fixture": PARITY_FIXTURE, "checked": False, "why": "fixture missing"}
+    want = dict(np.load(path))
+    idx = [int(i) for i in want["indices"]]
+    bad = []
+    for s, i in enumerate(idx):
+        o = batch.oscillation(0, i)
+        got = {"state": batch.state(i), "amps": o["amps"], "pers": o["pers"], "avg_peak": o["avg_peak"],
+               "ncrit": o["ncrit"]}
+        for k, v in got.items():
+            w = want[("state_%d" if k == "state" else "a0_" + k + "_%d") % s]
+            a, b = np.asarray(v, np.float64), np.asarray(w, np.float64)
+            if a.shape != b.shape or not np.array_equal(np.isnan(a), np.isnan(b)) or \
+                    not np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)]):
+                bad.append("set %d %s" % (i, k))
+    return {"fixture": PARITY_FIXTURE, "checked": True, "sets": idx, "bit_exact": not bad, "mismatches": bad,
+            "what": "final state and mh1 oscillation amplitudes, periods, mean peaks and critical-point counts of "
+                    "these sets after the timed run, against DENSE's own outputs"}
+
+
 def cpu_sample(kind_pref="reference", num_sets=8, minutes=300.0, seed=7):
     """DENSE (or the oracle port) on the host, one core, a bounded sample:
     `num_sets` sets of the workload for `minutes` simulated minutes."""
@@ -596,6 +624,11 @@ def main():
     chunks, _ = batch.progress()
     status = batch.status()
     done_cell_steps = int(sum(int(chunks[i]) * 10 * sets[i].num_cells for i in range(len(sets))))
+    # the timed run's results against DENSE's own on the workload's sets
+    # it holds (the default workload on rank 0 only)
+    parity = None
+    if (rank == 0 and a.sets == 4096 and a.minutes == 1200.0 and analyses and precision == E.FP64):
+        parity = batch_parity(batch)
     t = torch.tensor([total_ms, done_cell_steps], dtype=torch.float64, device="cuda")
     if world > 1:
         tm = t.clone()
@@ -672,6 +705,7 @@ def main():
             "clocks": clk,
             "step_ms": {"min": min(step_ms), "max": max(step_ms)},
             "status_nonzero_sets": int((status != 0).sum()),
+            "parity": parity,
         }
         print(json.dumps(line), flush=True)
     batch.close()

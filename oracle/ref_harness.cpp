@@ -16,7 +16,12 @@
 // headers with `private`/`protected` mapped to `public`.
 //
 // ConcentrationCheck (measurement/conccheck.hpp) does not compile against
-// the current DENSE headers, so oracle_add_conccheck returns -1 here.
+// the current DENSE headers (it derives from the old non-template Analysis
+// and calls a constructor that no longer exists), so the harness carries
+// its bound test (conccheck.hpp:25-51) on the current Analysis<Sim>
+// interface, applied to the state of DENSE's own Deterministic_Simulation,
+// and oracle_run drops a set the way run_simulation does
+// (run_simulation.hpp:131-150).
 
 // Standard headers first, so only DENSE's own classes see the access remap.
 #include <algorithm>
@@ -50,6 +55,7 @@
 #include "sim/determ/determ.hpp"
 #include "measurement/oscillation.hpp"
 #include "measurement/basic.hpp"
+#include "measurement/bad_simulation_error.hpp"
 #include "model_impl.hpp"
 #undef private
 #undef protected
@@ -59,8 +65,42 @@ using Sim = Deterministic_Simulation;
 
 namespace {
 
+// ConcentrationCheck::update and check (conccheck.hpp:25-51) as they are
+// worded there: every cell of [min, max), the target species or (target -1)
+// every species; a concentration below the lower or above the upper bound
+// throws Bad_Simulation_Error for the simulation.
+class HarnessConcCheck : public Analysis<Sim> {
+ public:
+  HarnessConcCheck(std::vector<Species> const& sp, dense::Natural cmin, dense::Natural cmax, Real lo, Real hi,
+                   Real t0, Real t1, int target)
+      : Analysis<Sim>(sp, {cmin, cmax}, {t0, t1}), lower_bound(lo), upper_bound(hi), target_specie(target) {}
+
+  void update(Sim& simulation, std::ostream&) override {
+    for (unsigned c = min; c < max; ++c) {
+      if (target_specie > -1) {
+        check(simulation, c, static_cast<Species>(target_specie));
+      } else {
+        for (dense::Natural s = 0; s < NUM_SPECIES; ++s) check(simulation, c, static_cast<Species>(s));
+      }
+    }
+  }
+  void finalize() override {}
+  HarnessConcCheck* clone() const override { return new HarnessConcCheck(*this); }
+  dense::Details get_details() override { return dense::Details(); }
+
+ private:
+  void check(Sim& simulation, dense::Natural cell, Species species) const {
+    Real concentration = simulation.get_concentration(cell, species);
+    if (concentration < lower_bound || concentration > upper_bound)
+      throw dense::Bad_Simulation_Error<Sim>("Concentration out of bounds", simulation);
+  }
+
+  Real lower_bound, upper_bound;
+  int target_specie;
+};
+
 struct Entry {
-  int kind;  // 0 basic, 1 oscillation
+  int kind;  // 0 basic, 1 oscillation, 2 concentration check
   std::unique_ptr<Analysis<Sim>> a;
 };
 
@@ -165,14 +205,25 @@ int oracle_add_oscillation(void* p, int n, const int* species, int cmin, int cma
   return static_cast<int>(h->analyses.size() - 1);
 }
 
-int oracle_add_conccheck(void*, int, int, int, double, double, double, double) { return -1; }
+int oracle_add_conccheck(void* p, int target, int cmin, int cmax, double lo, double hi, double t0, double t1) {
+  Harness* h = static_cast<Harness*>(p);
+  std::vector<Species> sp;
+  if (target >= 0) sp.push_back(static_cast<Species>(target));
+  h->analyses.push_back(Entry{2, std::unique_ptr<Analysis<Sim>>(
+      new HarnessConcCheck(sp, cmin, cmax, lo, hi, t0, t1, target))});
+  return static_cast<int>(h->analyses.size() - 1);
+}
 
 void oracle_steps(void* p, long n) {
   Harness* h = static_cast<Harness*>(p);
   for (long i = 0; i < n; ++i) h->sim->step();
 }
 
-// run_simulation's loop for one simulation (run_simulation.hpp:127-163).
+// run_simulation's loop for one simulation (run_simulation.hpp:127-163):
+// every analysis is called back in each chunk, each inside its own try; a
+// Bad_Simulation_Error from any of them removes the simulation after the
+// chunk's callbacks (it is not aged again, and its analyses are neither
+// finalized nor shown), status 1.  Returns the chunks begun.
 long oracle_run(void* p, double duration, double interval) {
   Harness* h = static_cast<Harness*>(p);
   using D = std::chrono::duration<Real, std::chrono::minutes::period>;
@@ -181,7 +232,18 @@ long oracle_run(void* p, double duration, double interval) {
   Real analysis_chunks = dur / intvl;
   long a = 0;
   for (a = 0; a < analysis_chunks; a++) {
-    for (auto& e : h->analyses) e.a->when_updated_by(*h->sim, h->sink);
+    bool bad = false;
+    for (auto& e : h->analyses) {
+      try {
+        e.a->when_updated_by(*h->sim, h->sink);
+      } catch (dense::Bad_Simulation_Error<Sim>&) {
+        bad = true;
+      }
+    }
+    if (bad) {
+      h->status |= 1;
+      return a;
+    }
     h->sim->age_by(intvl);
     h->sink.str("");
   }

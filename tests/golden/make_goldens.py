@@ -10,11 +10,12 @@
    the output files it wrote.
 3. ``ref_<case>.npz``: full-precision outputs of DENSE itself (compiled from
    its sources into oracle/_ref/ by oracle/build.py and driven through
-   oracle/ref_harness.cpp) on the small cases of CASES below, together with
-   the inputs they were computed from.  The GPU tests compare the engine
-   with these on machines without the DENSE tree.
+   oracle/ref_harness.cpp) on the small cases of CASES and, named on the
+   command line, the full-size configurations of FULL_CASES (cases.py).
+   The GPU tests compare the engine with these on machines without the
+   DENSE tree.
 
-Usage: python tests/golden/make_goldens.py   (needs the DENSE tree)
+Usage: python tests/golden/make_goldens.py [case ...]   (needs the DENSE tree)
 """
 
 import os
@@ -161,44 +162,77 @@ def copy_ctest():
         shutil.copyfile(os.path.join(dense_dir(), src), os.path.join(out, dst))
 
 
-def run_ref(name):
+def _ref_set(args):
+    """DENSE's outputs for set `s` of case `name` (keys as in the fixtures)."""
+    name, s = args
     from oracle.pyoracle import load_ref
     case = build_case(name)
     R = load_ref(case["model"])
     if R is None:
         raise RuntimeError("DENSE harness not built")
+    ps = case["sets"][s]
     out = {}
-    for s, ps in enumerate(case["sets"]):
-        sim = R.create(ps["off"], ps["ids"], ps["cell_params"], ps["set_params"], ps["init_conc"], case["dt"],
-                       ps.get("perturb"))
-        for a in case["analyses"]:
-            if a["kind"] == "basic":
-                sim.add_basic(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1])
-            elif a["kind"] == "oscillation":
-                sim.add_oscillation(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1], a["win"],
-                                    a["intvl"])
-        out["chunks_%d" % s] = sim.run(ps["duration"], case["interval"])
-        out["state_%d" % s] = sim.state()
-        out["S_%d" % s] = sim.ring_sizes()[0]
-        for i, a in enumerate(case["analyses"]):
-            if a["kind"] == "basic":
-                b = sim.basic(i)
-                for k in ("mins", "sums", "maxs", "samples", "time"):
-                    out["a%d_%s_%d" % (i, k, s)] = np.asarray(b[k])
-                if a["cells"][0] == 0:
-                    for k in ("cell_mins", "cell_sums", "cell_maxs"):
-                        out["a%d_%s_%d" % (i, k, s)] = b[k]
-            elif a["kind"] == "oscillation":
-                o = sim.oscillation(i)
-                for k in ("amps", "pers", "avg_peak", "ncrit", "samples", "time"):
-                    out["a%d_%s_%d" % (i, k, s)] = np.asarray(o[k])
+    sim = R.create(ps["off"], ps["ids"], ps["cell_params"], ps["set_params"], ps["init_conc"], case["dt"],
+                   ps.get("perturb"))
+    for a in case["analyses"]:
+        if a["kind"] == "basic":
+            sim.add_basic(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1])
+        elif a["kind"] == "oscillation":
+            sim.add_oscillation(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1], a["win"],
+                                a["intvl"])
+        elif a["kind"] == "conccheck":
+            if sim.add_conccheck(a["target"], a["cells"][0], a["cells"][1], a["lo"], a["hi"], a["t"][0],
+                                 a["t"][1]) < 0:
+                raise RuntimeError("DENSE harness without a concentration check")
+    out["chunks_%d" % s] = sim.run(ps["duration"], case["interval"])
+    out["status_%d" % s] = np.int32(sim.status())
+    out["state_%d" % s] = sim.state()
+    out["S_%d" % s] = sim.ring_sizes()[0]
+    for i, a in enumerate(case["analyses"]):
+        if a["kind"] == "basic":
+            b = sim.basic(i)
+            for k in ("mins", "sums", "maxs", "samples", "time"):
+                out["a%d_%s_%d" % (i, k, s)] = np.asarray(b[k])
+            if a["cells"][0] == 0:
+                for k in ("cell_mins", "cell_sums", "cell_maxs"):
+                    out["a%d_%s_%d" % (i, k, s)] = b[k]
+        elif a["kind"] == "oscillation":
+            o = sim.oscillation(i)
+            for k in ("amps", "pers", "avg_peak", "ncrit", "samples", "time"):
+                out["a%d_%s_%d" % (i, k, s)] = np.asarray(o[k])
+    return out
+
+
+def run_ref(name):
+    """DENSE on every set of the case (sets in parallel host processes,
+    each DENSE single-threaded as it is)."""
+    import multiprocessing as mp
+    case = build_case(name)
+    n = len(case["sets"])
+    jobs = [(name, s) for s in range(n)]
+    if n > 1:
+        with mp.get_context("spawn").Pool(min(n, os.cpu_count() or 1)) as pool:
+            parts = pool.map(_ref_set, jobs)
+    else:
+        parts = [_ref_set(jobs[0])]
+    out = {}
+    for part in parts:
+        out.update(part)
+    if "indices" in case:
+        out["indices"] = np.asarray(case["indices"], np.int64)
     np.savez_compressed(os.path.join(HERE, "ref_%s.npz" % name), **out)
     print("ref_%s.npz" % name, len(out), "arrays")
 
 
 if __name__ == "__main__":
-    copy_ctest()
-    copy_inputs()
-    run_cli_cases()
-    for name in (sys.argv[1:] or list(CASES)):
-        run_ref(name)
+    # no arguments: the CTest files, the command-line cases and every small
+    # case; names (from CASES or FULL_CASES) regenerate just those fixtures
+    if len(sys.argv) > 1:
+        for name in sys.argv[1:]:
+            run_ref(name)
+    else:
+        copy_ctest()
+        copy_inputs()
+        run_cli_cases()
+        for name in CASES:
+            run_ref(name)

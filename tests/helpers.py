@@ -24,10 +24,13 @@ def run_oracle(lib, name):
         for a in case["analyses"]:
             if a["kind"] == "basic":
                 sim.add_basic(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1])
-            else:
+            elif a["kind"] == "oscillation":
                 sim.add_oscillation(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1], a["win"],
                                     a["intvl"])
+            else:
+                sim.add_conccheck(a["target"], a["cells"][0], a["cells"][1], a["lo"], a["hi"], a["t"][0], a["t"][1])
         out["chunks_%d" % s] = sim.run(ps["duration"], case["interval"])
+        out["status_%d" % s] = np.int32(sim.status())
         out["state_%d" % s] = sim.state()
         out["S_%d" % s] = sim.ring_sizes()[0]
         for i, a in enumerate(case["analyses"]):
@@ -38,7 +41,7 @@ def run_oracle(lib, name):
                 if a["cells"][0] == 0:
                     for k in ("cell_mins", "cell_sums", "cell_maxs"):
                         out["a%d_%s_%d" % (i, k, s)] = b[k]
-            else:
+            elif a["kind"] == "oscillation":
                 o = sim.oscillation(i)
                 for k in ("amps", "pers", "avg_peak", "ncrit", "samples", "time"):
                     out["a%d_%s_%d" % (i, k, s)] = np.asarray(o[k])
@@ -56,9 +59,13 @@ def run_engine(name, precision=0, graph=False, chunks_per_call=-1):
     for a in case["analyses"]:
         if a["kind"] == "basic":
             an.append(Analysis.basic(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1]))
-        else:
+        elif a["kind"] == "oscillation":
             an.append(Analysis.oscillation(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1],
                                            a["win"], a["intvl"]))
+        else:
+            # DENSE's check takes one target species, or every species (-1)
+            an.append(Analysis.conccheck([a["target"]] if a["target"] >= 0 else [], a["cells"][0], a["cells"][1],
+                                         a["lo"], a["hi"], a["t"][0], a["t"][1]))
     b = Batch(case["model"], sets, case["dt"], case["interval"], an, precision=precision)
     if chunks_per_call < 0:
         b.run(-1, graph=graph)
@@ -83,7 +90,7 @@ def run_engine(name, precision=0, graph=False, chunks_per_call=-1):
                 if a["cells"][0] == 0:
                     for k in ("cell_mins", "cell_sums", "cell_maxs"):
                         out["a%d_%s_%d" % (i, k, s)] = r[k]
-            else:
+            elif a["kind"] == "oscillation":
                 r = b.oscillation(i, s)
                 for k in ("amps", "pers", "avg_peak", "ncrit", "samples", "time"):
                     out["a%d_%s_%d" % (i, k, s)] = np.asarray(r[k])

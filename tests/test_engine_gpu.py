@@ -13,8 +13,10 @@ from tests.helpers import load_fixture, mismatches, run_engine, run_oracle
 
 pytestmark = pytest.mark.gpu
 
-EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init", "turing", "nan_test", "delay_reaction",
-               "bz", "briggs_rauscher"]
+# her_pert_factors: -b perturbation factors resize DENSE's rings
+# (base.cpp:55-140), moving the rows that zero-truncated delays read (lag S-1)
+EXACT_CASES = ["her_test", "her_pert", "her_sets", "her_delays", "her_init", "her_pert_factors", "turing", "nan_test",
+               "delay_reaction", "bz", "briggs_rauscher"]
 
 
 @pytest.mark.parametrize("name", EXACT_CASES)
@@ -158,28 +160,25 @@ def test_nan_parameter_rejects_only_that_set():
     assert ch[1] == 0 and ch[0] == 300
 
 
-def test_concentration_check_drops_like_the_oracle():
+def test_concentration_check_drops_like_dense():
     """ConcentrationCheck (conccheck.hpp:25-51) with run_simulation's drop
-    (run_simulation.hpp:131-150): the set stops at the first chunk whose
-    sample leaves the bounds."""
+    (run_simulation.hpp:131-150), against DENSE's own Deterministic_Simulation
+    with that check (tests/golden/ref_her_conccheck.npz): four sets leave
+    mh1's bounds in the first 15 minutes at different chunks, two leave the
+    all-species bounds of cells 4-11 at minute 20, two run to the end; each
+    dropped set stops at the chunk whose sample failed, with DENSE's state
+    and Basic accumulators at that point."""
+    want = load_fixture("her_conccheck")
+    got = run_engine("her_conccheck")
+    assert sorted(int(want["status_%d" % s]) for s in range(8)) == [0, 0, 1, 1, 1, 1, 1, 1]
+    for s in range(8):
+        assert (int(got["status_%d" % s]) & E.SET_DROPPED) == int(want["status_%d" % s])
+        got["status_%d" % s] = np.int32(int(got["status_%d" % s]) & E.SET_DROPPED)
+    assert mismatches(want, got) == []
+    # a check whose bounds hold keeps every set
     from dense_b200 import workloads
-    from dense_b200.tissue import default_graph
-    from oracle.pyoracle import load_oracle
     p = workloads.template_params()
     mh1 = workloads.her_species("mh1")[0]
-    b = _her_batch([p, p], analyses=[E.Analysis.conccheck([mh1], 0, 16, 0.0, 30.0)])
-    b.run()
-    b.sync()
-    st = b.status()
-    ch, age = b.progress()
-    O = load_oracle("her_model_2014")
-    off, ids = default_graph(16, 4)
-    sim = O.create(off, ids, np.tile(p, (16, 1)), p, None, 0.01)
-    sim.add_conccheck(mh1, 0, 16, 0.0, 30.0)
-    a = sim.run(30.0, 0.1)
-    assert sim.status() & 1
-    assert st[0] & E.SET_DROPPED and st[1] & E.SET_DROPPED
-    assert ch[0] == a and ch[1] == a
     b2 = _her_batch([p], analyses=[E.Analysis.conccheck([mh1], 0, 16, 0.0, 1e9)])
     b2.run()
     assert b2.status()[0] == 0
