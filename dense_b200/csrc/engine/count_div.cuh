@@ -1,30 +1,23 @@
-// Correctly rounded division by a divisor known ahead of its uses.
+// Division of a sum by a small neighbour count, correctly rounded.
 //
-// DENSE divides in the working precision: neighbour sums by their count
-// (determ.hpp:81-89) and concentrations by critical values that are constant
-// for a parameter set (her_model_2014's rates, model_impl.hpp:193-224).  The
-// engines must return exactly the IEEE round-to-nearest quotient RN(x/c).
-// For a divisor c > 0 with rc = RN(1/c) precomputed this computes
+// DENSE averages neighbour concentrations as sum / count in the working
+// precision (determ.hpp:81-89).  The engines must return exactly that
+// IEEE round-to-nearest quotient.  For a count c with rc = RN(1/c) this
+// computes
 //
 //   q0 = RN(x * rc),   r0 = x - q0*c (one FMA),   q1 = RN(q0 + r0*rc),
 //
-// Markstein's refinement of a quotient by one FMA step (P. Markstein,
-// "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Dev. 34(1), 1990), and then proves q1 = RN(x/c)
-// with the remainder r1 = RN(x - q1*c) (one FMA): q1 is the correctly
-// rounded quotient when x/c lies strictly inside q1's rounding interval,
-// i.e. |x - q1*c| < h*c with h half the gap between q1 and its neighbours.
-// For a q1 that is not a power of two, h = p * 2^-(m+1) where p = 2^e is
-// q1's leading power of two (its exponent bits alone) and m the mantissa
-// width, so h*c = p * cg with cg = c * 2^-(m+1), an exact product while it
-// stays in the normal range.  The test |r1| < p * cg is sound even when r1
-// is rounded: rounding is monotone and p * cg is representable, so |r1| <
-// p * cg implies |x - q1*c| < p * cg.  Whenever the proof does not go
-// through (q1 a power of two, zero, subnormal, inf or NaN; p * cg not
-// normal; a tie; a refinement that missed) the plain division x / c is
-// returned instead, so the result always equals x / c.  A divisor outside
-// [2^-900, 2^900] (2^-100, 2^100 in FP32), or not positive, gets rc = cg =
-// 0, which makes the proof fail and every quotient take the division.
+// Markstein's refinement of a quotient by one FMA step (P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990), and then proves q1 = RN(x/c) with the exact remainder
+// r1 = x - q1*c: q1 is the correctly rounded quotient exactly when x/c lies
+// strictly inside q1's rounding interval, i.e. |r1| < c * (half the gap to
+// q1's neighbour on r1's side).  The remainder of a quotient within a few
+// ulps of x/c is a small multiple of ulp(q1) and so exactly representable,
+// and c times a power of two is exact.  Whenever the proof does not go
+// through (a tie, an operand outside the normal range, zero, inf, NaN) the
+// plain division x / c is returned instead, so the result always equals
+// x / c.
 #pragma once
 
 #include <cmath>
@@ -110,68 +103,29 @@ DENSE_HD inline T cd_abs(T a) {
 #endif
 }
 
-template <typename T>
-struct DivConst;
-
-template <>
-struct DivConst<double> {
-  static constexpr double kGap = 0x1p-53;       // 2^-(m+1)
-  static constexpr double kLo = 0x1p-900, kHi = 0x1p+900;
-  static constexpr double kMinNormal = 0x1p-1022;
-  static constexpr uint64_t kExp = 0x7FF0000000000000ull, kMant = 0x000FFFFFFFFFFFFFull;
-};
-
-template <>
-struct DivConst<float> {
-  static constexpr float kGap = 0x1p-24f;
-  static constexpr float kLo = 0x1p-100f, kHi = 0x1p+100f;
-  static constexpr float kMinNormal = 0x1p-126f;
-  static constexpr uint32_t kExp = 0x7F800000u, kMant = 0x007FFFFFu;
-};
-
-// q = x / c proven correctly rounded without the division; false when the
-// proof does not go through (q is then undefined).  rc = RN(1/c), cg = c *
-// 2^-(m+1); see above.
-template <typename T>
-DENSE_HD inline bool div_proved_try(T x, T c, T rc, T cg, T& q) {
-  using Tr = CountDivTraits<T>;
-  using K = DivConst<T>;
-  const T q0 = x * rc;
-  const T r0 = cd_fma(-q0, c, x);
-  const T q1 = cd_fma(r0, rc, q0);
-  const T r1 = cd_fma(-q1, c, x);
-  const typename Tr::Bits b = Tr::bits(q1);
-  const T lim = Tr::from(b & K::kExp) * cg;  // h * c
-  q = q1;
-  return (b & K::kMant) != 0 && cd_abs(r1) < lim && lim > K::kMinNormal;
-}
-
-// x / c for c > 0 with rc = RN(1/c) and cg = c * 2^-(m+1) (both 0 when c is
-// outside the quick range); always equal to x / c.
-template <typename T>
-DENSE_HD inline T div_proved(T x, T c, T rc, T cg) {
-  T q;
-  if (div_proved_try(x, c, rc, cg, q)) return q;
-  return x / c;
-}
-
-// rc and cg of a divisor, or zeros when c is outside the quick range.
-template <typename T>
-DENSE_HD inline void quick_divisor(T c, T& rc, T& cg) {
-  using K = DivConst<T>;
-  if (c >= K::kLo && c <= K::kHi) {
-    rc = T(1) / c;
-    cg = c * K::kGap;
-  } else {
-    rc = T(0);
-    cg = T(0);
-  }
-}
-
-// x / c for an integer-valued count c >= 1, with rc = RN(1/c).
+// x / c for an integer-valued c >= 1, with rc = RN(1/c); see above.
 template <typename T>
 DENSE_HD inline T div_by_count(T x, T c, T rc) {
-  return div_proved(x, c, rc, c * DivConst<T>::kGap);
+  using Tr = CountDivTraits<T>;
+  using Bits = typename Tr::Bits;
+  const T ax = cd_abs(x);
+  if (ax >= Tr::kLo && ax <= Tr::kHi) {
+    const T q0 = x * rc;
+    const T r0 = cd_fma(-q0, c, x);
+    const T q1 = cd_fma(r0, rc, q0);
+    const T r1 = cd_fma(-q1, c, x);  // exact
+    const Bits b = Tr::bits(q1);
+    const Bits expo = (b >> Tr::kMant) & ((Bits(1) << (sizeof(T) * 8 - 1 - Tr::kMant)) - 1);
+    const bool pow2 = (b & ((Bits(1) << Tr::kMant) - 1)) == 0;
+    // half the gap to the neighbour away from zero: 2^(e - kMant - 1), as a
+    // biased exponent expo - kMant - 1; towards zero it halves again when
+    // |q1| is a power of two
+    const T up = Tr::from((expo - Tr::kMant - 1) << Tr::kMant);
+    const T down = pow2 ? up * T(0.5) : up;
+    const bool away = (r1 > T(0)) == (q1 > T(0));
+    if (cd_abs(r1) < (away ? up : down) * c) return q1;
+  }
+  return x / c;
 }
 
 }  // namespace dense_b200

@@ -16,7 +16,6 @@ constexpr int kNS = NUM_SPECIES;
 constexpr int kNR = NUM_REACTIONS;
 constexpr int kND = NUM_DELAY_REACTIONS;
 constexpr int kNP = NUM_PARAMS;
-constexpr int kNC = NUM_CRITICAL_SPECIES;
 constexpr int kMaxAnalyses = 8;
 constexpr int kStepThreads = 256;  // register kernel: one thread per cell, one CTA per set
 constexpr int kMaxCells = 65536;   // memory kernel: cells per set

@@ -25,8 +25,6 @@
 
 #include <cuda_runtime.h>
 
-#include <type_traits>
-
 #include "count_div.cuh"
 #include "engine_types.hpp"
 
@@ -43,45 +41,6 @@ struct DelayArg {
   int dr;
   int k;
   __device__ __forceinline__ operator T() const { return prm[(kNR + dr) * pstride]; }
-};
-
-// A set's critical value and its reciprocal RN(1/c) (0 when c is outside
-// the quick-division range), kept in shared memory by the kernels of sets
-// whose cells share one parameter row.
-template <typename T>
-struct __align__(2 * sizeof(T)) CritPair {
-  T c, rc;
-};
-
-template <typename T>
-__device__ __forceinline__ void fill_crit_table(const T* s_prm, CritPair<T>* s_crit, int tid, int nthreads) {
-  for (int i = tid; i < kNC; i += nthreads) {
-    const T c = s_prm[kNR + kND + i];
-    T rc, cg;
-    quick_divisor(c, rc, cg);
-    s_crit[i] = CritPair<T>{c, rc};
-  }
-}
-
-// What getCritVal returns (Context::getCritVal, sim/base.hpp:393-397): the
-// critical value, which converts to the number itself.  With kQuick it also
-// carries RN(1/c), and `x / value` for x of the working precision -- how
-// DENSE's models use it (her_model_2014, model_impl.hpp:193-224) -- takes
-// div_proved's refined quotient instead of the division instruction
-// sequence; the quotient is IEEE's either way.  Other operand types divide
-// as the plain number would.
-template <typename T, bool kQuick>
-struct CritArg {
-  T c, rc;
-  __device__ __forceinline__ operator T() const { return c; }
-  friend __device__ __forceinline__ T operator/(T x, const CritArg& a) {
-    return kQuick ? div_proved(x, a.c, a.rc, a.c * DivConst<T>::kGap) : x / a.c;
-  }
-  template <typename U, typename = typename std::enable_if<std::is_arithmetic<U>::value &&
-                                                           !std::is_same<U, T>::value>::type>
-  friend __device__ __forceinline__ auto operator/(U x, const CritArg& a) -> decltype(x / a.c) {
-    return x / a.c;
-  }
 };
 
 // Neighbour counts whose reciprocals the memory kernel keeps in a table.
@@ -109,7 +68,6 @@ struct DeviceContext {
   T rc;                    // RN(1 / nnbr)
   const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
   const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
-  const CritPair<T>* crit; // kUniform: critical values and reciprocals [NC] (shared)
   bool ordered;            // the set runs in cell-dependency levels (memory kernel)
   int n_cells;
   int cell;
@@ -209,13 +167,7 @@ struct DeviceContext {
     return DelayArg<T>{prm, pstride, static_cast<int>(d),
                        kd ? kd[d * kd_stride] : static_cast<int>(prm[(kNR + d) * pstride])};
   }
-  __device__ __forceinline__ CritArg<T, kUniform> getCritVal(critspecie_id c) const {
-    if (kUniform) {
-      const CritPair<T> q = crit[c];
-      return CritArg<T, kUniform>{q.c, q.rc};
-    }
-    return CritArg<T, kUniform>{prm[(kNR + kND + c) * pstride], T(0)};
-  }
+  __device__ __forceinline__ T getCritVal(critspecie_id c) const { return prm[(kNR + kND + c) * pstride]; }
 };
 
 // ------------------------------------------------------------ analyses
@@ -575,7 +527,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   __shared__ int s_flags;
   __shared__ double s_samples[kMaxAnalyses];
   __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
-  __shared__ CritPair<T> s_crit[kNC > 0 ? kNC : 1];
 
   const int set = set_list[blockIdx.x];
   const SetDesc& sd = a.sets[set];
@@ -623,7 +574,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
       s_olag[i] = ol;
       s_nlag[i] = nl;
     }
-    fill_crit_table(s_prm, s_crit, c, blk);
   }
   int* s_kd = reinterpret_cast<int*>(s_dyn + (a.n_analyses > 0 ? a.n_vals * blk : 0));
   int* s_csr = s_kd + kND * blk;
@@ -671,7 +621,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const 
   }
   DeviceContext<T, kUniform> ctx{cur,  prm,    ps,   s_kd + cell, blk,    s_S,    lmask, lroff, ring,
                                  static_cast<int>(step), nbr, nnbr, T(1) / static_cast<T>(nnbr), lolag, lnlag,
-                                 s_crit, false, n, cell, &err};
+                                 false, n, cell, &err};
 
   const T dt = static_cast<T>(a.dt);
   int chunk = pg.chunk;
@@ -826,7 +776,6 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
   __shared__ int s_olag[kND > 0 ? kND * kNS : 1], s_nlag[kND > 0 ? kND * kNS : 1];
   __shared__ T* s_rows[kNS];
   __shared__ T* s_crows[kNS];
-  __shared__ CritPair<T> s_crit[kNC > 0 ? kNC : 1];
 
   const int set = set_list[blockIdx.x];
   const SetDesc& sd = a.sets[set];
@@ -851,10 +800,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
   double* anl = a.anl + sd.anl_base;
   if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
   __syncthreads();
-  if (kUniform) {
-    fill_lag_tables(s_prm, s_S, s_mask, s_olag, s_nlag, tid, blk);
-    fill_crit_table(s_prm, s_crit, tid, blk);
-  }
+  if (kUniform) fill_lag_tables(s_prm, s_S, s_mask, s_olag, s_nlag, tid, blk);
   __syncthreads();
 
   T* ring = static_cast<T*>(a.ring) + sd.ring_base;
@@ -910,7 +856,7 @@ __global__ void __launch_bounds__(256, 2) dense_step_mem_kernel(const StepArgs a
           DeviceContext<T, kUniform> ctx{cur,    prm,    ps,     nullptr, 0,      s_S,  s_mask, s_roff,
                                          ring,   st32,   a.nbr_idx + nb0, cnt,
                                          cnt < kRcTable ? s_rc[cnt] : T(1) / static_cast<T>(cnt),
-                                         s_olag, s_nlag, s_crit, ordered, n,      cell,   &err};
+                                         s_olag, s_nlag, ordered, n,      cell,   &err};
           T dsp[kNS];
 #pragma unroll
           for (int sp = 0; sp < kNS; ++sp) dsp[sp] = T(0);
@@ -994,7 +940,6 @@ struct WaveContext {
   T rc;                    // RN(1 / nnbr)
   const int* olag;         // kUniform: own-read lag table [ND][NS] (shared)
   const int* nlag;         // kUniform: neighbour-read lag table [ND][NS] (shared)
-  const CritPair<T>* crit; // kUniform: critical values and reciprocals [NC] (shared)
   int n_cells;
   int cell;
   int* err;
@@ -1089,13 +1034,7 @@ struct WaveContext {
   __device__ __forceinline__ DelayArg<T> getDelay(delay_reaction_id d) const {
     return DelayArg<T>{prm, pstride, static_cast<int>(d), static_cast<int>(prm[(kNR + d) * pstride])};
   }
-  __device__ __forceinline__ CritArg<T, kUniform> getCritVal(critspecie_id c) const {
-    if (kUniform) {
-      const CritPair<T> q = crit[c];
-      return CritArg<T, kUniform>{q.c, q.rc};
-    }
-    return CritArg<T, kUniform>{prm[(kNR + kND + c) * pstride], T(0)};
-  }
+  __device__ __forceinline__ T getCritVal(critspecie_id c) const { return prm[(kNR + kND + c) * pstride]; }
 };
 
 // The wave kernel: one CTA per ordered set (neighbour reads of the row
@@ -1121,7 +1060,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
   __shared__ T* s_rows[kNS];
   __shared__ T* s_crows[kNS];
   __shared__ T s_rc[kWaveMaxNbrs + 1];  // RN(1 / count)
-  __shared__ CritPair<T> s_crit[kNC > 0 ? kNC : 1];
 
   const int set = set_list[blockIdx.x];
   const SetDesc& sd = a.sets[set];
@@ -1192,7 +1130,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
       s_olag[i] = ol;
       s_nlag[i] = nl;
     }
-    fill_crit_table(s_prm, s_crit, tid, blk);
   }
   __syncthreads();
 
@@ -1281,7 +1218,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
           const T* prm = pstride == 0 ? s_prm : P + cell;
           const int ps = pstride == 0 ? 1 : n;
           WaveContext<T, kUniform> ctx{cur,    prm,    ps, lS,   lD,   r0,  lbase, lw, nb, cnt, s_rc[cnt],
-                                       s_olag, s_nlag, s_crit, n,  cell, &err};
+                                       s_olag, s_nlag, n,  cell, &err};
           T dsp[kNS];
 #pragma unroll
           for (int sp = 0; sp < kNS; ++sp) dsp[sp] = T(0);

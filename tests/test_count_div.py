@@ -1,7 +1,5 @@
-"""The engines' correctly rounded divisions (csrc/engine/count_div.cuh) --
-by a neighbour count, and by a divisor with a precomputed reciprocal such
-as a parameter set's critical value -- equal IEEE division, checked on the
-host."""
+"""The engines' correctly rounded division by a neighbour count
+(csrc/engine/count_div.cuh) equals IEEE division, checked on the host."""
 
 import os
 import subprocess
@@ -12,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ENGINE = os.path.join(os.path.dirname(HERE), "dense_b200", "csrc", "engine")
 
 
-def test_quick_divisions_match_ieee_division(tmp_path):
+def test_div_by_count_matches_ieee_division(tmp_path):
     exe = str(tmp_path / "count_div_check")
     r = subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", ENGINE,
                         os.path.join(HERE, "native", "count_div_check.cpp"), "-o", exe],
