@@ -170,15 +170,59 @@ def targets(F):
     return np.nan_to_num(T).astype(np.float32), M.astype(np.float32)
 
 
-def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, group=None, device=0):
-    """The MLP surrogate on (P, F); with a process group, data-parallel over
-    the ranks' shards (gradients averaged every step)."""
+class Surrogate:
+    """The trained networks behind one predict(): every output is trained
+    standardised (minus its mean over the rows where it is defined, over
+    its standard deviation there) and mapped back on prediction; with
+    several networks (an ensemble of different initial weights and batch
+    orders) their outputs are averaged."""
+
+    def __init__(self, nets, mu, sd):
+        self.nets, self.mu, self.sd = nets, np.asarray(mu, np.float32), np.asarray(sd, np.float32)
+        self.dev = nets[0].dev
+
+    def predict(self, X):
+        y = sum(n.predict(X) for n in self.nets) / len(self.nets)
+        return y * self.sd + self.mu
+
+    def predict_device(self, x):
+        import torch
+        y = sum(n.predict_device(x) for n in self.nets) / len(self.nets)
+        return y * torch.as_tensor(self.sd, device=y.device) + torch.as_tensor(self.mu, device=y.device)
+
+
+def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, group=None, device=0, ensemble=1):
+    """The MLP surrogate on (P, F): `ensemble` networks trained on
+    standardised targets; with a process group, data-parallel over the
+    ranks' shards (gradients averaged every step)."""
     from .surrogate import MLP
     X = encode(P)
     T, M = targets(F)
-    net = MLP(X.shape[1], T.shape[1], seed=seed, lr=lr, group=group, device=device)
-    net.fit(X, T, M, epochs=epochs, batch=min(batch, (X.shape[0] // 128) * 128), seed=seed, log=log)
-    return net
+    mu = np.zeros(T.shape[1], np.float32)
+    sd = np.ones(T.shape[1], np.float32)
+    for j in range(3):  # log period, log amplitude, synchrony; the indicators stay 0/1
+        on = M[:, j] > 0
+        if on.sum() > 1:
+            mu[j] = float(T[on, j].mean())
+            sd[j] = max(1e-6, float(T[on, j].std()))
+    if group is not None:
+        # the same scaling on every rank: the mean of the ranks' statistics
+        import torch
+        import torch.distributed as dist
+        t = torch.as_tensor(np.concatenate([mu, sd]), dtype=torch.float64)
+        if dist.get_backend(group) == "nccl":
+            t = t.cuda(device)
+        dist.all_reduce(t, group=group)
+        t = (t / dist.get_world_size(group)).cpu().numpy().astype(np.float32)
+        mu, sd = t[:T.shape[1]], t[T.shape[1]:]
+    Ts = ((T - mu) / sd) * M
+    nets = []
+    for k in range(ensemble):
+        net = MLP(X.shape[1], T.shape[1], seed=seed + 1000 * k, lr=lr, group=group, device=device)
+        net.fit(X, Ts, M, epochs=epochs, batch=min(batch, (X.shape[0] // 128) * 128), seed=seed + 1000 * k,
+                log=log)
+        nets.append(net)
+    return Surrogate(nets, mu, sd)
 
 
 def predicted_score(pred):

@@ -13,7 +13,16 @@
 
 Prints one JSON object.  Usage:
   python -m dense_b200.search_run [--train N] [--test N] [--candidates N]
-      [--minutes M] [--cells C] [--epochs E] [--generations G]
+      [--minutes M] [--resim-minutes R[,R2...]] [--cells C] [--epochs E]
+      [--generations G]
+
+--minutes is the horizon of the training and held-out simulations (the
+features' window is 0-60 min, and the first 60 minutes of a run do not
+depend on what follows); --resim-minutes the horizons at which the search
+simulates its candidates -- the screened survivors and the plain-search
+sample alike -- the first one reported as "search", each one also under
+"search_by_horizon" with the same trained network and candidates (default
+1200 min, the configuration's horizon, and 60 min beside it).
 
 Under torchrun (one process per GPU) steps 1, 2 and 4 shard: each rank
 simulates its share of the training candidates, the surrogate trains
@@ -55,9 +64,13 @@ def main(argv=None):
     ap.add_argument("--candidates", type=int, default=1000000)
     ap.add_argument("--keep", type=float, default=0.01)
     ap.add_argument("--plain-sample", type=int, default=4096)
-    ap.add_argument("--minutes", type=float, default=60.0, help="simulated minutes (the feature window is 0-60)")
+    ap.add_argument("--minutes", type=float, default=60.0,
+                    help="simulated minutes of the training data (the feature window is 0-60)")
+    ap.add_argument("--resim-minutes", default="1200,60",
+                    help="simulated minutes of the search's simulations, comma-separated")
     ap.add_argument("--cells", type=int, default=200)
     ap.add_argument("--epochs", type=int, default=150)
+    ap.add_argument("--ensemble", type=int, default=1, help="networks averaged by the surrogate")
     ap.add_argument("--generations", type=int, default=3)
     ap.add_argument("--seed", type=int, default=100)
     a = ap.parse_args(argv)
@@ -77,12 +90,20 @@ def main(argv=None):
                    "oscillating_fraction": float(F_train["oscillates"].mean()),
                    "accepted_fraction": float(S.accepted(F_train).mean())}
     t1 = time.perf_counter()
-    net = S.train_surrogate(P_train, F_train, epochs=a.epochs, batch=2048, seed=a.seed, log=log)
+    net = S.train_surrogate(P_train, F_train, epochs=a.epochs, batch=2048, seed=a.seed, log=log,
+                            ensemble=a.ensemble)
     res["training_s"] = time.perf_counter() - t1
     res["held_out_error"] = S.feature_errors(net, P_test, F_test)
-    res["search"] = S.screened_search(net, a.candidates, a.seed + 2, keep=a.keep, plain_sample=a.plain_sample,
-                                      sim_kwargs=sim, log=log)
-    res["search_with_one_time_cost"] = with_one_time_cost(res)
+    res["search_by_horizon"] = {}
+    for k, m in enumerate(float(x) for x in str(a.resim_minutes).split(",")):
+        r = S.screened_search(net, a.candidates, a.seed + 2, keep=a.keep, plain_sample=a.plain_sample,
+                              sim_kwargs=dict(sim, minutes=m), log=log)
+        r["minutes"] = m
+        r["with_one_time_cost"] = with_one_time_cost(dict(res, search=r))
+        res["search_by_horizon"]["%g" % m] = r
+        if k == 0:
+            res["search"] = r
+            res["search_with_one_time_cost"] = r["with_one_time_cost"]
     if a.generations > 0:
         fit = lambda X: S.search_fitness(S.simulate_features(S.decode(X), **sim))  # noqa: E731
         pred = lambda X: S.predicted_score(net.predict(X.astype(np.float32)))  # noqa: E731
@@ -117,10 +138,11 @@ def sharded(a, log):
     res["data"] = {"train_sets": a.train, "seconds_max_over_ranks": float(t.item())}
     t1 = time.perf_counter()
     net = S.train_surrogate(P, F, epochs=a.epochs, batch=2048, seed=a.seed, log=log if rank == 0 else None,
-                            group=dist.group.WORLD, device=local)
+                            group=dist.group.WORLD, device=local, ensemble=a.ensemble)
     res["training_s"] = time.perf_counter() - t1
     res["search"] = S.screened_search_sharded(net, a.candidates, a.seed + 2, keep=a.keep,
-                                              group=dist.group.WORLD, sim_kwargs=sim,
+                                              group=dist.group.WORLD,
+                                              sim_kwargs=dict(sim, minutes=float(str(a.resim_minutes).split(",")[0])),
                                               log=log if rank == 0 else None)
     res["total_s"] = time.perf_counter() - t0
     if rank == 0:
