@@ -6,7 +6,7 @@
 //   -s/--step-size <min>  -c/--cell-total <n> -w/--tissue-width <n> |
 //   -f/--cell-graph <file>  -d/--initial-conc <csv>  -a/--analysis <xml>
 //   -e/--data-export <csv>  -o/--specie-option <list>  -v/--time-col
-//   -N/--test-run  -n/--no-color  -h/--help
+//   -i/--data-import <csv>  -N/--test-run  -n/--no-color  -h/--help
 // plus --precision fp64|fp32 (FP32 rates with Kahan-compensated state) and
 // --device <ordinal>.
 //
@@ -363,6 +363,7 @@ void usage() {
                "[-p | --param-sets]    <string> Parameter sets CSV.\n"
                "[-b | --perturbations] <string|Real> Perturbation factors entering the history sizing.\n"
                "[-e | --data-export]   <string> Trajectory export CSV.\n"
+               "[-i | --data-import]   <string> Analyse a trajectory export instead of simulating (with -t, -u).\n"
                "[-o | --specie-option] <string> Species to export / analyse.\n"
                "[-a | --analysis]      <string> Analysis XML.\n"
                "[-c | --cell-total]       <int> Cells.\n"
@@ -379,133 +380,22 @@ void usage() {
 
 }  // namespace
 
-static int run_cli(int argc, char** argv) {
-  Args A;
-  A.v.assign(argv + 1, argv + argc);
-  if (A.has("h", "help") || A.has("H", "usage") || argc == 1) {
-    usage();
-    return EXIT_SUCCESS;
-  }
-  // DENSE flags outside this command: the stochastic seed (-r) and the
-  // colour switch (-n) change nothing here and are accepted; gradients (-g)
-  // are undefined in DENSE (simulation_width_ is 0 when gradient_index is
-  // taken modulo it, sim/base.cpp:22-31) and analysis of an imported
-  // trajectory (-i, io/csvr_sim.cpp) is not built, so both are refused
-  // rather than ignored
-  if (A.has("g", "gradients")) {
-    std::cout << "Error: [-g | --gradients] is not supported (DENSE's gradient path divides by the tissue width "
-                 "before it is set); give per-cell parameters instead.\n";
-    return EXIT_FAILURE;
-  }
-  if (A.has("i", "data-import")) {
-    std::cout << "Error: [-i | --data-import] (analysis of an imported trajectory) is not supported by this "
-                 "command.\n";
-    return EXIT_FAILURE;
-  }
-  dense_model_info mi;
-  dense_model_get_info(&mi);
-  const int NS = mi.num_species, NP = mi.num_params, NR = mi.num_reactions;
-
-  double time_total = 0, anlys_intvl = 0, step_size = 0;
-  std::string param_path;
-  bool ok = A.real("t", "time-total", &time_total);
-  ok = A.real("u", "anlys-intvl", &anlys_intvl) && ok;
-  ok = A.str("p", "param-sets", &param_path) && ok;
-  if (!ok) {
-    std::cout << "Error: Your current set of command line arguments produces a useless state. (No inputs are "
-                 "specified.)\n";
-    return EXIT_FAILURE;
-  }
-  if (!A.real("s", "step-size", &step_size) || step_size == 0.0) {
-    std::cout << "Error: the deterministic engine needs [-s | --step-size].\n";
-    return EXIT_FAILURE;
-  }
-  bool csv_ok;
-  std::vector<double> pvals = read_reals(param_path, &csv_ok);
-  if (!csv_ok) {
-    std::cout << "CSV file input failed. CSV file '" << param_path << "' not found or open.\n";
-    return EXIT_FAILURE;
-  }
-  if (pvals.size() % NP) {
-    std::cout << "ERROR: Partial set encountered at end of Parameter Sets CSV file.\n";
-    return EXIT_FAILURE;
-  }
-  const int num_sets = static_cast<int>(pvals.size() / NP);
-
-  // tissue (arg_parse.hpp:127-169)
-  int cells = 0, width = 0;
-  std::string graph_path;
-  bool c_flag = A.integer("c", "cell-total", &cells), w_flag = A.integer("w", "tissue-width", &width);
-  bool f_flag = A.str("f", "cell-graph", &graph_path);
-  Graph g;
-  if (w_flag && c_flag && !f_flag) {
-    if (cells <= 0 || width <= 0 || width > cells) {
-      std::cout << "Error: invalid cell total or tissue width.\n";
-      return EXIT_FAILURE;
-    }
-    g = default_graph(cells, width);
-  } else if (f_flag && !c_flag && !w_flag) {
-    bool gok = graph_path.find("graphml") != std::string::npos ? read_graphml(graph_path, &g)
-                                                              : read_edge_list(graph_path, &g);
-    if (!gok || g.out.empty()) {
-      std::cout << "Error: Cell graph from " << graph_path << " is invalid.\n";
-      return EXIT_FAILURE;
-    }
-    cells = static_cast<int>(g.out.size());
-  } else {
-    std::cout << "Error: Either specify a cell total with [-c | --cell-total] and a width with [-w | "
-                 "--tissue-width] or provide a cell graph file with [-f | --cell-graph].\n";
-    return EXIT_FAILURE;
-  }
-  std::vector<int> off{0}, ids;
-  for (auto& nb : g.out) {
-    for (int x : nb) ids.push_back(x);
-    off.push_back(static_cast<int>(ids.size()));
-  }
-
-  // initial concentrations (conc_vector, Sim_Initializer.hpp:138-157)
-  std::vector<double> conc;
-  std::string conc_path;
-  // (DENSE dereferences a failed reader here and crashes; the file must open)
-  if (A.str("d", "initial-conc", &conc_path)) {
-    conc = read_reals(conc_path, &csv_ok);
-    if (!csv_ok) {
-      std::cout << "CSV file input failed. CSV file '" << conc_path << "' not found or open.\n";
-      return EXIT_FAILURE;
-    }
-    conc.resize(NS, 0.0);
-  }
-  // -b: one global factor or a per-reaction CSV (history sizing only)
-  std::vector<double> pert;
-  std::string pb;
-  if (A.str("b", "perturbations", &pb)) {
-    char* end = nullptr;
-    double v = std::strtod(pb.c_str(), &end);
-    if (end && *end == 0) pert.assign(NR, v);
-    else {
-      pert = read_reals(pb, &csv_ok);
-      if (!csv_ok) {
-        std::cout << "CSV file input failed. CSV file '" << pb << "' not found or open.\n";
-        return EXIT_FAILURE;
-      }
-      pert.resize(NR, 0.0);
-    }
-  }
-
-  // analyses (parse_analysis_entries.hpp:64-126)
-  std::vector<Entry> entries;
+// The analyses of a run (parse_analysis_entries.hpp:64-126): analyses.xml
+// entries (-a), else the trajectory export (-e), else a Basic analysis of
+// every species and cell unless -N.  False when the XML cannot be read.
+static bool parse_entries(const Args& A, int cells, int NS, std::vector<Entry>* entries, bool* time_col) {
   std::string default_sp;
   A.str("o", "specie-option", &default_sp);
   std::string xml_path, export_path;
   // DENSE reads -v as a flag with a value (parse_analysis_entries.hpp:365):
   // it is on only when another argument follows it
   std::string time_col_arg;
-  bool time_col = A.str("v", "time-col", &time_col_arg);
+  *time_col = A.str("v", "time-col", &time_col_arg);
   if (A.str("a", "analysis", &xml_path)) {
     Node root;
     if (!parse_xml_file(xml_path, &root)) {
       std::cout << "Error: could not read analysis file " << xml_path << "\n";
-      return EXIT_FAILURE;
+      return false;
     }
     for (const Node& an : root.kids) {
       if (an.tag != "anlys") continue;
@@ -534,7 +424,7 @@ static int run_cli(int argc, char** argv) {
                   << ", outside the " << cells << "-cell tissue\n";
         continue;
       }
-      entries.push_back(e);
+      entries->push_back(e);
     }
   } else if (A.str("e", "data-export", &export_path) && !export_path.empty()) {
     Entry e;
@@ -546,7 +436,7 @@ static int run_cli(int argc, char** argv) {
     e.d.time_start = 0;
     e.d.time_end = INFINITY;
     e.out = export_path;
-    entries.push_back(e);
+    entries->push_back(e);
   } else if (!A.has("N", "test-run")) {
     std::cout << "Warning: performing basic analysis only.  Did you mean to use the [-e | --data-export] and/or "
                  "[-a | --analysis] flag(s)? (use -N to suppress this error)\n";
@@ -558,44 +448,15 @@ static int run_cli(int argc, char** argv) {
     e.d.cell_end = cells;
     e.d.time_start = 0;
     e.d.time_end = INFINITY;
-    entries.push_back(e);
+    entries->push_back(e);
   }
-  for (Entry& e : entries) {
-    e.d.num_species = static_cast<int>(e.species.size());
-    e.d.species = e.species.data();
-  }
-  std::vector<dense_analysis_desc> descs;
-  for (Entry& e : entries) descs.push_back(e.d);
+  return true;
+}
 
-  std::string prec = "fp64";
-  A.str("precision", "precision", &prec);
-  int device = 0;
-  A.integer("device", "device", &device);
-  std::vector<dense_set_desc> sets(num_sets);
-  for (int s = 0; s < num_sets; ++s) {
-    sets[s].num_cells = cells;
-    sets[s].nbr_offsets = off.data();
-    sets[s].nbr_ids = ids.data();
-    sets[s].set_params = pvals.data() + static_cast<size_t>(s) * NP;
-    sets[s].cell_params = nullptr;
-    sets[s].init_conc = conc.empty() ? nullptr : conc.data();
-    sets[s].perturb = pert.empty() ? nullptr : pert.data();
-    sets[s].duration = time_total;
-  }
-  dense_run_desc run{prec == "fp32" ? DENSE_FP32_KAHAN : DENSE_FP64, step_size, anlys_intvl,
-                     static_cast<int>(descs.size()), descs.data(), device};
-  dense_engine* eng = nullptr;
-  if (dense_engine_create(&run, num_sets, sets.data(), &eng) != DENSE_OK) {
-    std::cout << "Error: " << dense_last_error() << "\n";
-    return EXIT_FAILURE;
-  }
-  if (dense_engine_run(eng, -1, nullptr) != DENSE_OK || dense_engine_sync(eng) != DENSE_OK) {
-    std::cout << "Error: " << dense_last_error() << "\n";
-    return EXIT_FAILURE;
-  }
-  std::vector<int32_t> status(num_sets);
-  dense_engine_status(eng, status.data());
-
+// Every analysis' output of every set that was not dropped, as DENSE's
+// run_simulation shows them (run_simulation.hpp:113-121, 159-163).
+static void write_outputs(dense_engine* eng, const std::vector<Entry>& entries, int num_sets, int NS, bool time_col,
+                          const std::vector<int32_t>& status) {
   for (int s = 0; s < num_sets; ++s) {
     if (status[s] & DENSE_SET_DROPPED) continue;  // run_simulation drops bad sets (run_simulation.hpp:131-150)
     for (size_t ai = 0; ai < entries.size(); ++ai) {
@@ -692,6 +553,352 @@ static int run_cli(int argc, char** argv) {
       }
     }
   }
+}
+
+// A trajectory export (csvw_sim, io/csvw_sim.ipp:17-91: what -e writes)
+// read back for -i: the header row (cell-total, time-start, time-col,
+// cell-start, cell-end, one 0/1 flag per species), the row of column names
+// (the value columns' species in file order -- csvw_sim writes them in the
+// -o order -- after an optional Time and Cell column), then cell-end -
+// cell-start rows of values per sample.  Numbers are read as DENSE reads
+// them (strtold, then double).  samples is [k][NS][cell-total], NaN where
+// the file holds no value.
+struct Import {
+  int cells = 0, cell_start = 0, cell_end = 0, time_col = 0, k = 0;
+  double time_start = 0;
+  std::vector<int> species;  // value columns, file order
+  std::vector<double> samples;
+};
+
+static bool read_import(const std::string& path, int NS, Import* im, std::string* err) {
+  std::ifstream f(path);
+  if (!f) {
+    *err = "CSV file input failed. CSV file '" + path + "' not found or open.";
+    return false;
+  }
+  auto split = [](const std::string& ln) {
+    std::vector<std::string> out;
+    std::string cur;
+    for (char c : ln) {
+      if (c == ',') {
+        out.push_back(trim(cur));
+        cur.clear();
+      } else {
+        cur += c;
+      }
+    }
+    if (!trim(cur).empty()) out.push_back(trim(cur));
+    return out;
+  };
+  auto number = [](const std::string& t, double* v) {
+    char* end = nullptr;
+    const long double x = std::strtold(t.c_str(), &end);
+    *v = static_cast<double>(x);
+    return !t.empty() && end && *end == 0;
+  };
+  std::vector<std::string> body;
+  std::string ln;
+  while (std::getline(f, ln)) {
+    const std::string t = trim(ln);
+    if (!t.empty() && t[0] != '#') body.push_back(t);
+  }
+  if (body.size() < 3 || body[0].compare(0, 10, "cell-total") != 0) {
+    *err = "not a trajectory export (no cell-total header row): " + path;
+    return false;
+  }
+  const std::vector<std::string> head = split(body[1]);
+  if (static_cast<int>(head.size()) != 5 + NS) {
+    *err = "trajectory header has " + std::to_string(head.size()) + " fields, expected " + std::to_string(5 + NS);
+    return false;
+  }
+  std::vector<double> h(head.size());
+  for (size_t i = 0; i < head.size(); ++i)
+    if (!number(head[i], &h[i])) {
+      *err = "trajectory header field '" + head[i] + "' is not a number";
+      return false;
+    }
+  im->cells = static_cast<int>(h[0]);
+  im->time_start = h[1];
+  im->time_col = static_cast<int>(h[2]);
+  im->cell_start = static_cast<int>(h[3]);
+  im->cell_end = static_cast<int>(h[4]);
+  if (im->cells <= 0 || im->cell_start < 0 || im->cell_end > im->cells || im->cell_end <= im->cell_start) {
+    *err = "trajectory header's cell range is invalid";
+    return false;
+  }
+  std::vector<std::string> names = split(body[2]);
+  size_t skip = 0;
+  while (skip < names.size() && (names[skip] == "Time" || names[skip] == "Cell")) ++skip;
+  std::vector<bool> flagged(NS), seen(NS);
+  for (int i = 0; i < NS; ++i) flagged[i] = h[5 + i] != 0.0;
+  for (size_t j = skip; j < names.size(); ++j) {
+    int id = -1;
+    for (int i = 0; i < NS; ++i)
+      if (names[j] == dense_model_specie_name(i)) id = i;
+    if (id < 0 || !flagged[id] || seen[id]) {
+      *err = "trajectory column '" + names[j] + "' is not one of the header's species";
+      return false;
+    }
+    seen[id] = true;
+    im->species.push_back(id);
+  }
+  if (seen != flagged) {
+    *err = "trajectory columns do not match the header's species flags";
+    return false;
+  }
+  const int m = im->cell_end - im->cell_start, ncol = static_cast<int>(im->species.size());
+  std::vector<double> rows;
+  for (size_t r = 3; r < body.size(); ++r) {
+    std::vector<std::string> v = split(body[r]);
+    // the Time (and Cell) cells come first; only a sample's first row
+    // carries its time, the others leave the cell empty
+    if (v.size() == static_cast<size_t>(ncol) + skip) v.erase(v.begin(), v.begin() + skip);
+    else if (skip > 0 && v.size() + 1 == static_cast<size_t>(ncol) + skip && body[r][0] == ',')
+      v.erase(v.begin(), v.begin() + (skip - 1));
+    if (static_cast<int>(v.size()) != ncol) {
+      *err = "trajectory row " + std::to_string(r) + " holds " + std::to_string(v.size()) + " values, expected " +
+             std::to_string(ncol);
+      return false;
+    }
+    for (const std::string& t : v) {
+      double x;
+      if (!number(t, &x)) {
+        *err = "trajectory value '" + t + "' is not a number";
+        return false;
+      }
+      rows.push_back(x);
+    }
+  }
+  const size_t per = static_cast<size_t>(m) * ncol;
+  if (per == 0 || rows.size() % per) {
+    *err = "trajectory rows are not whole samples of " + std::to_string(m) + " cells";
+    return false;
+  }
+  im->k = static_cast<int>(rows.size() / per);
+  im->samples.assign(static_cast<size_t>(im->k) * NS * im->cells, NAN);
+  for (int k = 0; k < im->k; ++k)
+    for (int c = 0; c < m; ++c)
+      for (int j = 0; j < ncol; ++j)
+        im->samples[(static_cast<size_t>(k) * NS + im->species[j]) * im->cells + im->cell_start + c] =
+            rows[(static_cast<size_t>(k) * m + c) * ncol + j];
+  return true;
+}
+
+static int run_cli(int argc, char** argv) {
+  Args A;
+  A.v.assign(argv + 1, argv + argc);
+  if (A.has("h", "help") || A.has("H", "usage") || argc == 1) {
+    usage();
+    return EXIT_SUCCESS;
+  }
+  // DENSE flags outside this command: the stochastic seed (-r) and the
+  // colour switch (-n) change nothing here and are accepted; gradients (-g)
+  // are undefined in DENSE (simulation_width_ is 0 when gradient_index is
+  // taken modulo it, sim/base.cpp:22-31), so they are refused rather than
+  // ignored
+  if (A.has("g", "gradients")) {
+    std::cout << "Error: [-g | --gradients] is not supported (DENSE's gradient path divides by the tissue width "
+                 "before it is set); give per-cell parameters instead.\n";
+    return EXIT_FAILURE;
+  }
+  dense_model_info mi;
+  dense_model_get_info(&mi);
+  const int NS = mi.num_species, NP = mi.num_params, NR = mi.num_reactions;
+
+  // -i: analysis of an imported trajectory (main.cpp:160-175): no
+  // simulation; the analyses see the file's samples, one per chunk of -u
+  // minutes from the file's start time, for -t minutes (or as many samples
+  // as the file holds).  DENSE's own reader for it (CSV_Streamed_Simulation,
+  // io/csvr_sim.cpp:87-96) calls itself and never returns.
+  std::string import_path;
+  if (A.str("i", "data-import", &import_path)) {
+    double time_total = 0, anlys_intvl = 0;
+    if (!(A.real("t", "time-total", &time_total) && A.real("u", "anlys-intvl", &anlys_intvl)) ||
+        !(anlys_intvl > 0.0)) {
+      std::cout << "No time-total or anlys-intvl for CSV Simulation (fix in future)\n";
+      return EXIT_FAILURE;
+    }
+    Import im;
+    std::string err;
+    if (!read_import(import_path, NS, &im, &err)) {
+      std::cout << "Error: " << err << "\n";
+      return EXIT_FAILURE;
+    }
+    std::vector<Entry> entries;
+    bool time_col = false;
+    if (!parse_entries(A, im.cells, NS, &entries, &time_col)) return EXIT_FAILURE;
+    for (Entry& e : entries) {
+      for (int sp : e.species) {
+        bool held = false;
+        for (int x : im.species) held = held || x == sp;
+        if (!held) {
+          std::cout << "Error: the imported trajectory holds no " << dense_model_specie_name(sp) << "\n";
+          return EXIT_FAILURE;
+        }
+      }
+      if (e.d.cell_start < im.cell_start || e.d.cell_end > im.cell_end) {
+        std::cout << "Error: analysis of cells " << e.d.cell_start << "-" << e.d.cell_end
+                  << " outside the imported cells " << im.cell_start << "-" << im.cell_end << "\n";
+        return EXIT_FAILURE;
+      }
+      e.d.num_species = static_cast<int>(e.species.size());
+      e.d.species = e.species.data();
+    }
+    std::vector<dense_analysis_desc> descs;
+    for (Entry& e : entries) descs.push_back(e.d);
+    int device = 0;
+    A.integer("device", "device", &device);
+    // one set of the file's cells, no neighbours; its parameters are never used
+    std::vector<int> off(im.cells + 1, 0), ids(1, 0);
+    std::vector<double> prm(NP, 0.0);
+    dense_set_desc set{};
+    set.num_cells = im.cells;
+    set.nbr_offsets = off.data();
+    set.nbr_ids = ids.data();
+    set.set_params = prm.data();
+    set.duration = time_total;
+    dense_run_desc run{DENSE_FP64, anlys_intvl, anlys_intvl, static_cast<int>(descs.size()), descs.data(), device};
+    dense_engine* eng = nullptr;
+    const double chunks = std::ceil(time_total / anlys_intvl);  // run_simulation.hpp:127-130
+    const int k = static_cast<int>(std::min<double>(chunks, im.k));
+    if (dense_engine_create(&run, 1, &set, &eng) != DENSE_OK ||
+        dense_engine_analyze_samples(eng, 0, im.samples.data(), k, im.time_start) != DENSE_OK) {
+      std::cout << "Error: " << dense_last_error() << "\n";
+      return EXIT_FAILURE;
+    }
+    std::vector<int32_t> status(1);
+    dense_engine_status(eng, status.data());
+    write_outputs(eng, entries, 1, NS, time_col, status);
+    dense_engine_destroy(eng);
+    return EXIT_SUCCESS;
+  }
+
+  double time_total = 0, anlys_intvl = 0, step_size = 0;
+  std::string param_path;
+  bool ok = A.real("t", "time-total", &time_total);
+  ok = A.real("u", "anlys-intvl", &anlys_intvl) && ok;
+  ok = A.str("p", "param-sets", &param_path) && ok;
+  if (!ok) {
+    std::cout << "Error: Your current set of command line arguments produces a useless state. (No inputs are "
+                 "specified.)\n";
+    return EXIT_FAILURE;
+  }
+  if (!A.real("s", "step-size", &step_size) || step_size == 0.0) {
+    std::cout << "Error: the deterministic engine needs [-s | --step-size].\n";
+    return EXIT_FAILURE;
+  }
+  bool csv_ok;
+  std::vector<double> pvals = read_reals(param_path, &csv_ok);
+  if (!csv_ok) {
+    std::cout << "CSV file input failed. CSV file '" << param_path << "' not found or open.\n";
+    return EXIT_FAILURE;
+  }
+  if (pvals.size() % NP) {
+    std::cout << "ERROR: Partial set encountered at end of Parameter Sets CSV file.\n";
+    return EXIT_FAILURE;
+  }
+  const int num_sets = static_cast<int>(pvals.size() / NP);
+
+  // tissue (arg_parse.hpp:127-169)
+  int cells = 0, width = 0;
+  std::string graph_path;
+  bool c_flag = A.integer("c", "cell-total", &cells), w_flag = A.integer("w", "tissue-width", &width);
+  bool f_flag = A.str("f", "cell-graph", &graph_path);
+  Graph g;
+  if (w_flag && c_flag && !f_flag) {
+    if (cells <= 0 || width <= 0 || width > cells) {
+      std::cout << "Error: invalid cell total or tissue width.\n";
+      return EXIT_FAILURE;
+    }
+    g = default_graph(cells, width);
+  } else if (f_flag && !c_flag && !w_flag) {
+    bool gok = graph_path.find("graphml") != std::string::npos ? read_graphml(graph_path, &g)
+                                                              : read_edge_list(graph_path, &g);
+    if (!gok || g.out.empty()) {
+      std::cout << "Error: Cell graph from " << graph_path << " is invalid.\n";
+      return EXIT_FAILURE;
+    }
+    cells = static_cast<int>(g.out.size());
+  } else {
+    std::cout << "Error: Either specify a cell total with [-c | --cell-total] and a width with [-w | "
+                 "--tissue-width] or provide a cell graph file with [-f | --cell-graph].\n";
+    return EXIT_FAILURE;
+  }
+  std::vector<int> off{0}, ids;
+  for (auto& nb : g.out) {
+    for (int x : nb) ids.push_back(x);
+    off.push_back(static_cast<int>(ids.size()));
+  }
+
+  // initial concentrations (conc_vector, Sim_Initializer.hpp:138-157)
+  std::vector<double> conc;
+  std::string conc_path;
+  // (DENSE dereferences a failed reader here and crashes; the file must open)
+  if (A.str("d", "initial-conc", &conc_path)) {
+    conc = read_reals(conc_path, &csv_ok);
+    if (!csv_ok) {
+      std::cout << "CSV file input failed. CSV file '" << conc_path << "' not found or open.\n";
+      return EXIT_FAILURE;
+    }
+    conc.resize(NS, 0.0);
+  }
+  // -b: one global factor or a per-reaction CSV (history sizing only)
+  std::vector<double> pert;
+  std::string pb;
+  if (A.str("b", "perturbations", &pb)) {
+    char* end = nullptr;
+    double v = std::strtod(pb.c_str(), &end);
+    if (end && *end == 0) pert.assign(NR, v);
+    else {
+      pert = read_reals(pb, &csv_ok);
+      if (!csv_ok) {
+        std::cout << "CSV file input failed. CSV file '" << pb << "' not found or open.\n";
+        return EXIT_FAILURE;
+      }
+      pert.resize(NR, 0.0);
+    }
+  }
+
+  std::vector<Entry> entries;
+  bool time_col = false;
+  if (!parse_entries(A, cells, NS, &entries, &time_col)) return EXIT_FAILURE;
+  for (Entry& e : entries) {
+    e.d.num_species = static_cast<int>(e.species.size());
+    e.d.species = e.species.data();
+  }
+  std::vector<dense_analysis_desc> descs;
+  for (Entry& e : entries) descs.push_back(e.d);
+
+  std::string prec = "fp64";
+  A.str("precision", "precision", &prec);
+  int device = 0;
+  A.integer("device", "device", &device);
+  std::vector<dense_set_desc> sets(num_sets);
+  for (int s = 0; s < num_sets; ++s) {
+    sets[s].num_cells = cells;
+    sets[s].nbr_offsets = off.data();
+    sets[s].nbr_ids = ids.data();
+    sets[s].set_params = pvals.data() + static_cast<size_t>(s) * NP;
+    sets[s].cell_params = nullptr;
+    sets[s].init_conc = conc.empty() ? nullptr : conc.data();
+    sets[s].perturb = pert.empty() ? nullptr : pert.data();
+    sets[s].duration = time_total;
+  }
+  dense_run_desc run{prec == "fp32" ? DENSE_FP32_KAHAN : DENSE_FP64, step_size, anlys_intvl,
+                     static_cast<int>(descs.size()), descs.data(), device};
+  dense_engine* eng = nullptr;
+  if (dense_engine_create(&run, num_sets, sets.data(), &eng) != DENSE_OK) {
+    std::cout << "Error: " << dense_last_error() << "\n";
+    return EXIT_FAILURE;
+  }
+  if (dense_engine_run(eng, -1, nullptr) != DENSE_OK || dense_engine_sync(eng) != DENSE_OK) {
+    std::cout << "Error: " << dense_last_error() << "\n";
+    return EXIT_FAILURE;
+  }
+  std::vector<int32_t> status(num_sets);
+  dense_engine_status(eng, status.data());
+
+  write_outputs(eng, entries, num_sets, NS, time_col, status);
   dense_engine_destroy(eng);
   return EXIT_SUCCESS;
 }

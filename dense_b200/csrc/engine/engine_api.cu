@@ -185,7 +185,7 @@ int check_set(const dense_set_desc& in, const std::string& where) {
         return fail(DENSE_ERR_INVALID, where + "neighbour ids must ascend (DENSE keeps them in a std::set)");
     }
   }
-  if (in.schedule < DENSE_SCHEDULE_AUTO || in.schedule > DENSE_SCHEDULE_WAVE_GLOBAL)
+  if (in.schedule < DENSE_SCHEDULE_AUTO || in.schedule > DENSE_SCHEDULE_REGISTER)
     return fail(DENSE_ERR_INVALID, where + "unknown schedule hint");
   if (in.mem_block != 0 && (in.mem_block < 32 || in.mem_block > 256 || in.mem_block % 32))
     return fail(DENSE_ERR_INVALID, where + "mem_block must be 32..256, a multiple of 32");
@@ -268,7 +268,7 @@ int build_analyses(const dense_run_desc* run, int num_sets, const dense_set_desc
 }
 
 int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan, std::vector<double>& cell_params) {
-  const bool force_mem = in.schedule != DENSE_SCHEDULE_AUTO;
+  const bool force_mem = in.schedule != DENSE_SCHEDULE_AUTO && in.schedule != DENSE_SCHEDULE_REGISTER;
   const int n = in.num_cells;
   SetDesc& d = plan.d;
   d.n_cells = n;
@@ -306,7 +306,9 @@ int plan_set(const dense_set_desc& in, double dt, int elem_bytes, SetPlan& plan,
   plan_levels(in, ordered, plan);
   // the wave kernel takes ordered sets whose cells have at most
   // kWaveMaxNbrs neighbours and whose ids and level offsets fit 16 bits
-  if (ordered && in.schedule != DENSE_SCHEDULE_GLOBAL && n < 65536 &&
+  // (and, on request, sets without such reads: the wave kernel's rows in
+  // shared memory as far as they fit, one level per step)
+  if ((ordered || in.schedule == DENSE_SCHEDULE_SHARED_ROWS) && in.schedule != DENSE_SCHEDULE_GLOBAL && n < 65536 &&
       2 * static_cast<int64_t>(plan.lvl_off.size()) + 16 <= kWaveSmemBudget) {
     plan.wave = true;
     for (int c = 0; c < n; ++c)
@@ -640,6 +642,7 @@ int dense_engine_create(const dense_run_desc* run, int num_sets, const dense_set
       for (int i : reg_list) m = std::max(m, static_cast<double>(e->sets[i].n_chunks) * e->sets[i].steps_per_chunk);
       est.push_back({m, k++});
     }
+
     for (const auto& g : e->mem_groups) {
       double m = 0;
       for (int j = g[3]; j < g[3] + g[4]; ++j) {
@@ -1147,6 +1150,150 @@ int dense_graph_launch(void* graph_exec, void* stream) {
 
 int dense_graph_destroy(void* graph_exec) {
   if (graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph_exec));
+  return DENSE_OK;
+}
+
+// Analyses of imported samples (simulation -i): the set's analyses run over
+// the given sampled states instead of simulated ones.
+int dense_engine_analyze_samples(dense_engine* e, int set, const double* samples, int num_samples,
+                                 double time_start) {
+  NvtxRange range_("dense_engine_analyze_samples");
+  if (!e || set < 0 || set >= e->num_sets || num_samples < 0 || (num_samples > 0 && !samples))
+    return fail(DENSE_ERR_INVALID, "bad argument");
+  const StepArgs& a = e->args;
+  const int n = e->sets[set].n_cells;
+  // the samples in the rows of the kernels' sampled-state buffer: the
+  // species some analysis observes
+  const size_t per = static_cast<size_t>(std::max(1, a.n_vals)) * n;
+  std::vector<double> rows(per * std::max(1, num_samples), 0.0);
+  for (int k = 0; k < num_samples; ++k)
+    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+      if (a.val_slot[sp] >= 0)
+        std::memcpy(rows.data() + k * per + static_cast<size_t>(a.val_slot[sp]) * n,
+                    samples + (static_cast<size_t>(k) * NUM_SPECIES + sp) * n, sizeof(double) * n);
+  CUDA_TRY(cudaSetDevice(e->device));
+  DeviceBuffer d_rows;
+  int rc = d_rows.alloc(sizeof(double) * rows.size());
+  if (rc != DENSE_OK) return rc;
+  CUDA_TRY(cudaMemcpyAsync(d_rows.p, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(e->precision == DENSE_FP64
+               ? launch_import_fp64(a, set, static_cast<const double*>(d_rows.p), num_samples, time_start, e->stream)
+               : launch_import_fp32(a, set, static_cast<const double*>(d_rows.p), num_samples, time_start, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return DENSE_OK;
+}
+
+// ---- checkpoint / resume
+//
+// Snapshot layout: a CheckpointHeader, then the device blocks in the order
+// progress, state, history rings, analysis state.  The header carries the
+// block sizes and a hash of the batch's set descriptors and analyses, so a
+// snapshot is only accepted by an engine with the same layout.
+
+namespace {
+
+struct CheckpointHeader {
+  char magic[8];  // "DENSECK1"
+  int32_t precision, num_sets;
+  int64_t layout_hash;
+  int64_t bytes[4];
+};
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+CheckpointHeader checkpoint_header(const dense_engine* e) {
+  CheckpointHeader h{};
+  std::memcpy(h.magic, "DENSECK1", 8);
+  h.precision = e->precision;
+  h.num_sets = e->num_sets;
+  // the fields that place a set's run state in the four blocks (field by
+  // field: the structs' padding bytes are not initialised)
+  uint64_t x = 1469598103934665603ull;
+  auto mix = [&x](const void* p, size_t n) { x = fnv1a(x, p, n); };
+  for (const SetDesc& d : e->sets) {
+    mix(&d.n_cells, sizeof d.n_cells);
+    mix(&d.n_chunks, sizeof d.n_chunks);
+    mix(&d.steps_per_chunk, sizeof d.steps_per_chunk);
+    mix(&d.cell_base, sizeof d.cell_base);
+    mix(&d.ring_base, sizeof d.ring_base);
+    mix(&d.anl_base, sizeof d.anl_base);
+    mix(d.S, sizeof d.S);
+    mix(d.D, sizeof d.D);
+    mix(d.ring_off, sizeof d.ring_off);
+  }
+  for (const AnalysisDesc& A : e->analyses) {
+    mix(&A.kind, sizeof A.kind);
+    mix(&A.nsp, sizeof A.nsp);
+    mix(A.sp, sizeof(int) * A.nsp);
+    mix(&A.cmin, sizeof A.cmin);
+    mix(&A.cmax, sizeof A.cmax);
+    mix(&A.range_steps, sizeof A.range_steps);
+    mix(&A.off, sizeof A.off);
+  }
+  h.layout_hash = static_cast<int64_t>(x);
+  const DeviceBuffer* blocks[4] = {&e->d_prog, &e->d_state, &e->d_ring, &e->d_anl};
+  for (int i = 0; i < 4; ++i) h.bytes[i] = static_cast<int64_t>(blocks[i]->bytes);
+  return h;
+}
+
+}  // namespace
+
+int dense_engine_checkpoint_size(dense_engine* e, int64_t* bytes) {
+  if (!e || !bytes) return fail(DENSE_ERR_INVALID, "null argument");
+  const CheckpointHeader h = checkpoint_header(e);
+  *bytes = static_cast<int64_t>(sizeof h) + h.bytes[0] + h.bytes[1] + h.bytes[2] + h.bytes[3];
+  return DENSE_OK;
+}
+
+int dense_engine_checkpoint(dense_engine* e, void* buf, int64_t bytes) {
+  NvtxRange range_("dense_engine_checkpoint");
+  int64_t need = 0;
+  if (!e || !buf) return fail(DENSE_ERR_INVALID, "null argument");
+  dense_engine_checkpoint_size(e, &need);
+  if (bytes < need) return fail(DENSE_ERR_INVALID, "checkpoint buffer smaller than dense_engine_checkpoint_size");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  const CheckpointHeader h = checkpoint_header(e);
+  unsigned char* out = static_cast<unsigned char*>(buf);
+  std::memcpy(out, &h, sizeof h);
+  size_t off = sizeof h;
+  const DeviceBuffer* blocks[4] = {&e->d_prog, &e->d_state, &e->d_ring, &e->d_anl};
+  for (int i = 0; i < 4; ++i) {
+    if (h.bytes[i] > 0) CUDA_TRY(cudaMemcpy(out + off, blocks[i]->p, h.bytes[i], cudaMemcpyDeviceToHost));
+    off += h.bytes[i];
+  }
+  return DENSE_OK;
+}
+
+int dense_engine_restore(dense_engine* e, const void* buf, int64_t bytes) {
+  NvtxRange range_("dense_engine_restore");
+  if (!e || !buf) return fail(DENSE_ERR_INVALID, "null argument");
+  CheckpointHeader got;
+  if (bytes < static_cast<int64_t>(sizeof got)) return fail(DENSE_ERR_INVALID, "checkpoint shorter than its header");
+  std::memcpy(&got, buf, sizeof got);
+  const CheckpointHeader want = checkpoint_header(e);
+  if (std::memcmp(got.magic, want.magic, 8) != 0) return fail(DENSE_ERR_INVALID, "not a dense_b200 checkpoint");
+  if (got.precision != want.precision || got.num_sets != want.num_sets || got.layout_hash != want.layout_hash ||
+      std::memcmp(got.bytes, want.bytes, sizeof got.bytes) != 0)
+    return fail(DENSE_ERR_INVALID, "checkpoint of a batch with another layout (sets, analyses or precision)");
+  int64_t need = 0;
+  dense_engine_checkpoint_size(e, &need);
+  if (bytes < need) return fail(DENSE_ERR_INVALID, "checkpoint truncated");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  const unsigned char* in = static_cast<const unsigned char*>(buf) + sizeof got;
+  DeviceBuffer* blocks[4] = {&e->d_prog, &e->d_state, &e->d_ring, &e->d_anl};
+  for (int i = 0; i < 4; ++i) {
+    if (want.bytes[i] > 0) CUDA_TRY(cudaMemcpy(blocks[i]->p, in, want.bytes[i], cudaMemcpyHostToDevice));
+    in += want.bytes[i];
+  }
   return DENSE_OK;
 }
 

@@ -59,7 +59,6 @@ enum OscField : int {
   kOscTm2, kOscTm1,                 // times of critical points ncrit-3 and ncrit-2
   kOscPeakSum, kOscTroughSum, kOscNumPeaks, kOscNumTroughs, kOscCycleSum, kOscCycles,
   kOscAmp, kOscPer, kOscAvgPeak,    // results, written by finalize
-  kOscHi, kOscLo, kOscExtValid,     // window max/min while valid (1), else rescanned
   kOscFields
 };
 

@@ -277,35 +277,21 @@ __device__ __forceinline__ void osc_add_crit(const OscRef& o, double t, double c
 // is processed; loaded and stored as one batch of independent accesses.
 struct OscQueue {
   long start, end, current, live;
-  bool ext_valid;
-  double hi, lo;
   __device__ __forceinline__ void load(const OscRef& o) {
     const double s0 = o.f(kOscStart), e0 = o.f(kOscEnd), c0 = o.f(kOscCurrent), l0 = o.f(kOscLive);
-    const double v0 = o.f(kOscExtValid), h0 = o.f(kOscHi), w0 = o.f(kOscLo);
     start = static_cast<long>(s0);
     end = static_cast<long>(e0);
     current = static_cast<long>(c0);
     live = static_cast<long>(l0);
-    ext_valid = v0 != 0.0;
-    hi = h0;
-    lo = w0;
   }
   __device__ __forceinline__ void store(const OscRef& o) const {
     o.f(kOscStart) = static_cast<double>(start);
     o.f(kOscEnd) = static_cast<double>(end);
     o.f(kOscCurrent) = static_cast<double>(current);
     o.f(kOscLive) = static_cast<double>(live);
-    o.f(kOscExtValid) = ext_valid ? 1.0 : 0.0;
-    o.f(kOscHi) = hi;
-    o.f(kOscLo) = lo;
   }
-  // Queue::dequeue.  The value leaves the multiset; if it was the window's
-  // max or min the cached extremes are dropped and the next check rescans.
-  __device__ __forceinline__ void dequeue(const double* win, int m, int w) {
-    if (ext_valid) {
-      const double v = win[static_cast<size_t>(start) * m];
-      if (v == hi || v == lo) ext_valid = false;
-    }
+  // Queue::dequeue (the value leaves DENSE's multiset too)
+  __device__ __forceinline__ void dequeue(int w) {
     start = (start == w - 1) ? 0 : start + 1;
     if (2 * q_size(start, end, w) <= w) {
       current = current + 1;
@@ -315,47 +301,47 @@ struct OscQueue {
   }
 };
 
-// OscillationAnalysis::checkCritPoint (oscillation.ipp:110-119).  The
-// window max/min are those of the live values (DENSE keeps them in a
-// multiset).  A middle index of -1 (DENSE reads contents[-1]) or an empty
-// window gives no critical point.
-__device__ __forceinline__ void osc_check(const OscRef& o, OscQueue& q, const double* win, int m, int w,
+// OscillationAnalysis::checkCritPoint (oscillation.ipp:110-119): the middle
+// value is a peak when it equals the window's maximum and not its minimum,
+// a trough when it equals the minimum -- that is, a peak when no live value
+// lies above it and some lies below, a trough when none lies below.  The
+// window is scanned from both ends inwards, four values from each end at a
+// time, and the scan stops as soon as values above and below have both been
+// seen, so only an extreme middle value costs a whole pass.  A middle index
+// of -1 (DENSE reads contents[-1]), an empty window or a NaN middle value
+// gives no critical point; NaN values in the window compare neither above
+// nor below (DENSE keeps them in a std::multiset, whose order NaN breaks).
+__device__ __forceinline__ void osc_check(const OscRef& o, const OscQueue& q, const double* win, int m, int w,
                                           double samples, const AnalysisDesc& A) {
   if (q.current < 0 || q.live <= 0) return;
   const double mid = win[static_cast<size_t>(q.current) * m];
-  if (!q.ext_valid) {
-    // rescan in queue order; the loads of eight entries are issued before
-    // they are folded, so their latencies overlap
-    long idx = q.start;
-    double hi = win[static_cast<size_t>(idx) * m], lo = hi;
-    long k = 1;
-    for (; k + 8 <= q.live; k += 8) {
-      double x[8];
+  if (isnan(mid)) return;
+  bool above = false, below = false;
+  long lo = q.start, hi = q.end;  // oldest and newest live slots
+  long left = q.live;             // live values not yet looked at
+  while (left > 0 && !(above && below)) {
+    // slots past the live values hold mid, which is neither above nor below
+    double x[8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        idx = (idx == w - 1) ? 0 : idx + 1;
-        x[u] = win[static_cast<size_t>(idx) * m];
-      }
+    for (int u = 0; u < 4; ++u) {
+      const bool a0 = left > 2 * u, a1 = left > 2 * u + 1;
+      x[2 * u] = a0 ? win[static_cast<size_t>(lo) * m] : mid;
+      x[2 * u + 1] = a1 ? win[static_cast<size_t>(hi) * m] : mid;
+      if (a0) lo = (lo == w - 1) ? 0 : lo + 1;
+      if (a1) hi = (hi == 0) ? w - 1 : hi - 1;
+    }
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        hi = (hi < x[u]) ? x[u] : hi;
-        lo = (x[u] < lo) ? x[u] : lo;
-      }
+    for (int u = 0; u < 8; ++u) {
+      above = above || (x[u] > mid);
+      below = below || (x[u] < mid);
     }
-    for (; k < q.live; ++k) {
-      idx = (idx == w - 1) ? 0 : idx + 1;
-      const double x = win[static_cast<size_t>(idx) * m];
-      hi = (hi < x) ? x : hi;
-      lo = (x < lo) ? x : lo;
-    }
-    q.hi = hi;
-    q.lo = lo;
-    q.ext_valid = true;
+    left -= 8;
   }
+  if (above && below) return;
   double t = (samples - static_cast<double>(A.range_steps / 2)) * A.interval + A.t0;
   t = (0.0 < t) ? t : 0.0;
-  if (mid == q.hi && mid != q.lo) osc_add_crit(o, t, mid, true);
-  else if (mid == q.lo) osc_add_crit(o, t, mid, false);
+  if (!above && below) osc_add_crit(o, t, mid, true);
+  else if (!below) osc_add_crit(o, t, mid, false);
 }
 
 __device__ __forceinline__ OscRef osc_ref(double* st, const AnalysisDesc& A, int i, int cc) {
@@ -388,15 +374,11 @@ __device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& 
     q.end = (q.end == w - 1) ? 0 : q.end + 1;
     win[static_cast<size_t>(q.end) * m] = added;
     q.live += 1;
-    if (q.ext_valid) {
-      q.hi = (q.hi < added) ? added : q.hi;
-      q.lo = (added < q.lo) ? added : q.lo;
-    }
     if (2 * q_size(q.start, q.end, w) >= w) {
       q.current = q.current + 1;
       if (q.current == w) q.current = 0;
     }
-    if (q_size(q.start, q.end, w) == A.range_steps + 1) q.dequeue(win, m, w);
+    if (q_size(q.start, q.end, w) == A.range_steps + 1) q.dequeue(w);
     const bool stop = q_size(q.start, q.end, w) < A.range_steps / 2;
     if (!stop) osc_check(o, q, win, m, w, samples, A);
     q.store(o);
@@ -422,7 +404,7 @@ __device__ __forceinline__ void osc_cell_finalize(double* st, const AnalysisDesc
     q.load(o);
     for (;;) {
       if (!(q_size(q.start, q.end, w) >= (A.range_steps / 2) && q.live > 0)) break;
-      q.dequeue(win, m, w);
+      q.dequeue(w);
       osc_check(o, q, win, m, w, samples, A);
       samples += 1.0;
     }
@@ -1291,6 +1273,64 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_wave_kernel(c
   }
 }
 
+// Analysis of imported samples (simulation -i): the set's analyses see
+// `num_samples` sampled states read from `samples` ([sample][slot][cell],
+// the rows of the sampled-state buffer) instead of simulated ones, at the
+// ages time_start, time_start + interval, ... (accumulated as DENSE's
+// age_by does), then the oscillation analyses are finalized.  One CTA runs
+// the one set `set`; a failed concentration check stops it as a drop.
+struct ImportVals {
+  const double* base;
+  int n;
+  __device__ __forceinline__ double operator()(int slot, int cell) const { return base[slot * n + cell]; }
+};
+
+// (T: the batch's precision; the analyses work in double either way)
+template <typename T>
+__global__ void dense_import_kernel(const StepArgs a, int set, const double* samples, int num_samples,
+                                    double time_start) {
+  __shared__ double s_samples[kMaxAnalyses];
+  __shared__ int s_flags;
+  const SetDesc& sd = a.sets[set];
+  const int n = sd.n_cells;
+  const int tid = threadIdx.x, blk = blockDim.x;
+  double* anl = a.anl + sd.anl_base;
+  if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+  if (tid == 0) s_flags = 0;
+  __syncthreads();
+  double age = time_start;
+  int k = 0;
+  bool dropped = false;
+  for (; k < num_samples; ++k) {
+    const ImportVals vals{samples + static_cast<size_t>(k) * a.n_vals * n, n};
+    const bool bad = analyses_sample(a, anl, vals, tid, tid, blk, n, age, s_samples);
+    if (bad) atomicOr(&s_flags, 1);
+    __syncthreads();
+    if (tid < a.n_analyses) s_samples[tid] = anl[a.analyses[tid].off];
+    if (s_flags & 1) {
+      dropped = true;
+      break;
+    }
+    age += a.interval;
+  }
+  __syncthreads();
+  if (!dropped) {
+    for (int ai = 0; ai < a.n_analyses; ++ai) {
+      const AnalysisDesc& A = a.analyses[ai];
+      if (A.kind == kOscillation)
+        for (int c = tid; c < n; c += blk) osc_cell_finalize(anl + A.off, A, c, s_samples[ai]);
+    }
+  }
+  if (tid == 0) {
+    SetProgress out = a.prog[set];
+    out.chunk = k;
+    out.age = age;
+    out.status |= dropped ? kSetDropped : 0;
+    out.finalized = dropped ? 0 : 1;
+    a.prog[set] = out;
+  }
+}
+
 // Fills every set's state, history rows and analysis state with their
 // initial values: all rows of every ring hold the initial concentrations
 // (determ.cpp:42-51, zeros when none are given), Basic minima start at
@@ -1355,6 +1395,17 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
 
 }  // namespace dense_b200
 
+// Streaming multiprocessors of the current device (looked up once).
+inline int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+      n = v;
+  }
+  return n > 0 ? n : 148;
+}
+
 // Launchers, named by the including translation unit's precision suffix.
 #define DENSE_B200_STEP_VARIANT(T, KAHAN, THREADS, BLOCKS, UNIFORM, SMEM_CAP)                     \
   {                                                                                             \
@@ -1385,6 +1436,11 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
     dense_init_kernel<T><<<a.num_sets, 256, 0, s>>>(a, init_conc, init_status);                  \
     return cudaGetLastError();                                                                  \
   }                                                                                             \
+  cudaError_t launch_import_##SUFFIX(const StepArgs& a, int set, const double* samples, int num_samples, \
+                                     double time_start, cudaStream_t s) {                       \
+    dense_import_kernel<T><<<1, 256, 0, s>>>(a, set, samples, num_samples, time_start);         \
+    return cudaGetLastError();                                                                  \
+  }                                                                                             \
   cudaError_t launch_step_mem_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets,       \
                                        int block, cudaStream_t s) {                             \
     if (n_sets <= 0) return cudaSuccess;                                                        \
@@ -1412,7 +1468,9 @@ __global__ void dense_init_kernel(const StepArgs a, const double* init_conc, con
   cudaError_t launch_step_##SUFFIX(const StepArgs& a, const int* set_list, int n_sets, size_t smem, \
                                    cudaStream_t s) {                                            \
     if (n_sets <= 0) return cudaSuccess;                                                        \
-    if (a.block_threads <= 224) {                                                               \
+    /* two 224-thread CTAs per SM (128 registers) when the sets fill more  \
+       than one CTA per SM; else one CTA per SM with every register */     \
+    if (a.block_threads <= 224 && n_sets > sm_count()) {                                        \
       if (a.uniform_params) DENSE_B200_STEP_VARIANT(T, KAHAN, 224, 2, true, 100000)              \
       else DENSE_B200_STEP_VARIANT(T, KAHAN, 224, 2, false, 100000)                               \
     } else {                                                                                    \

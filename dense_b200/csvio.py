@@ -78,3 +78,64 @@ def read_init_conc(text, num_species):
     or zero-padded to num_species."""
     vals = read_reals(text)[:num_species]
     return vals + [0.0] * (num_species - len(vals))
+
+
+def _number(cell):
+    v, ok = _strtold_to_double(cell.strip())
+    if not ok or not cell.strip():
+        raise ValueError("not a number: %r" % cell)
+    return v
+
+
+def read_trajectory(text, species_names):
+    """A trajectory export (csvw_sim, io/csvw_sim.ipp:17-91: what
+    ``simulation -e`` writes) as the samples the analyses of ``simulation
+    -i`` see.
+
+    The header row gives cell-total, time-start, time-col, cell-start,
+    cell-end and one 0/1 flag per species; the row of column names gives
+    the value columns' species in file order (csvw_sim writes them in the
+    -o order, not by species id), after an optional Time (and Cell) column;
+    then each sample is cell-end - cell-start rows of values, one row per
+    cell.  Numbers are read as DENSE reads them (strtold, then double).
+    Returns (header dict, samples [k][num_species][cell_total]) with NaN for
+    species and cells the file does not hold."""
+    import numpy as np
+    lines = [ln.strip() for ln in text.splitlines()]
+    body = [ln for ln in lines if ln and not ln.startswith("#")]
+    if len(body) < 3 or not body[0].startswith("cell-total"):
+        raise ValueError("not a trajectory export: no cell-total header row")
+    head = [x for x in body[1].split(",") if x.strip()]
+    nsp = len(species_names)
+    if len(head) != 5 + nsp:
+        raise ValueError("trajectory header has %d fields, expected %d" % (len(head), 5 + nsp))
+    nums = [_number(x) for x in head]
+    cells, t0, time_col, cs, ce = int(nums[0]), nums[1], int(nums[2]), int(nums[3]), int(nums[4])
+    names = [x.strip() for x in body[2].split(",") if x.strip()]
+    skip = 0
+    while names and names[0] in ("Time", "Cell"):
+        names.pop(0)
+        skip += 1
+    cols = [species_names.index(nm) for nm in names]
+    flagged = sorted(i for i in range(nsp) if nums[5 + i] != 0.0)
+    if sorted(cols) != flagged:
+        raise ValueError("trajectory columns %s do not match the header's species flags" % names)
+    m = ce - cs
+    rows = []
+    for ln in body[3:]:
+        cellsv = ln.split(",")
+        if cellsv and cellsv[-1].strip() == "":
+            cellsv = cellsv[:-1]
+        vals = cellsv[skip:]
+        if len(vals) != len(cols):
+            raise ValueError("trajectory row with %d values, expected %d: %r" % (len(vals), len(cols), ln))
+        rows.append([_number(v) for v in vals])
+    if m <= 0 or len(rows) % m:
+        raise ValueError("trajectory rows (%d) are not whole samples of %d cells" % (len(rows), m))
+    k = len(rows) // m
+    out = np.full((k, nsp, cells), np.nan)
+    R = np.asarray(rows, np.float64).reshape(k, m, len(cols))
+    for j, sp in enumerate(cols):
+        out[:, sp, cs:ce] = R[:, :, j]
+    return {"cell_total": cells, "time_start": t0, "time_col": time_col, "cell_start": cs, "cell_end": ce,
+            "species": cols}, out

@@ -33,6 +33,8 @@ SCHEDULE_MEMORY = 1
 SCHEDULE_GLOBAL = 2
 SCHEDULE_SHARED_NEIGHBOUR = 3
 SCHEDULE_WAVE_GLOBAL = 4
+SCHEDULE_SHARED_ROWS = 5
+SCHEDULE_REGISTER = 6
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
@@ -90,6 +92,10 @@ _FUNCS = {
     "dense_engine_read_trajectory": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, C.c_int, _I]),
     "dense_engine_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _I]),
     "dense_engine_ring_info": (C.c_int, [C.c_void_p, C.c_int, _I, _I]),
+    "dense_engine_analyze_samples": (C.c_int, [C.c_void_p, C.c_int, _D, C.c_int, C.c_double]),
+    "dense_engine_checkpoint_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "dense_engine_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "dense_engine_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "dense_engine_destroy": (C.c_int, [C.c_void_p]),
 }
 
@@ -372,6 +378,29 @@ class Batch:
         bt = C.c_int()
         self.L._check(self.L.lib.dense_engine_info(self.h, C.byref(cs), C.byref(nb), C.byref(bt)))
         return dict(total_cell_steps=cs.value, device_bytes=nb.value, block_threads=bt.value)
+
+    def analyze_samples(self, set_index, samples, time_start=0.0):
+        """Runs the set's analyses over imported samples [k][species][cells]
+        (simulation -i) instead of simulating; read the results as after a
+        run."""
+        x = np.ascontiguousarray(samples, np.float64)
+        k = x.shape[0] if x.ndim == 3 else 0
+        self.L._check(self.L.lib.dense_engine_analyze_samples(self.h, set_index, _dp(x), k, float(time_start)))
+
+    def checkpoint(self):
+        """The batch's whole run state so far, as bytes (waits for the
+        engine's work): restore() on a Batch built from the same inputs --
+        in this process or another -- continues from exactly this point."""
+        n = C.c_int64()
+        self.L._check(self.L.lib.dense_engine_checkpoint_size(self.h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self.L._check(self.L.lib.dense_engine_checkpoint(self.h, buf.ctypes.data_as(C.c_void_p), n.value))
+        return buf.tobytes()
+
+    def restore(self, snapshot):
+        """Puts a checkpoint() of a batch with the same layout back."""
+        buf = np.frombuffer(snapshot, np.uint8)
+        self.L._check(self.L.lib.dense_engine_restore(self.h, buf.ctypes.data_as(C.c_void_p), buf.size))
 
     def ring_info(self, set_index):
         S = np.zeros(self.L.num_species, np.int32)

@@ -171,9 +171,10 @@ def targets(F):
 
 
 class Surrogate:
-    """The trained networks behind one predict(): every output is trained
-    standardised (minus its mean over the rows where it is defined, over
-    its standard deviation there) and mapped back on prediction; with
+    """The trained networks behind one predict(): every output (the 0/1
+    indicators included) is trained standardised (minus its mean over the
+    rows where it is defined, over its standard deviation there) and mapped
+    back on prediction; with
     several networks (an ensemble of different initial weights and batch
     orders) their outputs are averaged."""
 
@@ -200,7 +201,7 @@ def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, grou
     T, M = targets(F)
     mu = np.zeros(T.shape[1], np.float32)
     sd = np.ones(T.shape[1], np.float32)
-    for j in range(3):  # log period, log amplitude, synchrony; the indicators stay 0/1
+    for j in range(T.shape[1]):  # indicators too: rare acceptances then weigh as much as the rest
         on = M[:, j] > 0
         if on.sum() > 1:
             mu[j] = float(T[on, j].mean())

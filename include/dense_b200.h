@@ -70,6 +70,10 @@ extern "C" {
 #define DENSE_SCHEDULE_SHARED_NEIGHBOUR 3  /* as MEMORY, but only neighbour-read species in shared memory */
 #define DENSE_SCHEDULE_WAVE_GLOBAL 4       /* as MEMORY, but rows and cell records in global memory: more
                                               sets per SM (single-warp CTAs up to 32 per SM) */
+#define DENSE_SCHEDULE_SHARED_ROWS 5       /* a set without in-order neighbour reads in the wave kernel: its
+                                              history rows in shared memory as far as they fit, one level
+                                              per step */
+#define DENSE_SCHEDULE_REGISTER 6          /* register kernel (one thread per cell) */
 
 /* arithmetic of a batch */
 #define DENSE_FP64 0        /* matches DENSE's CPU path bit for bit */
@@ -172,6 +176,37 @@ DENSE_API int dense_engine_sync(dense_engine* e);
 /* Reset every set to its initial state (same inputs; no reallocation; in
    DENSE a new Simulation object). */
 DENSE_API int dense_engine_reset(dense_engine* e, void* stream);
+
+/* Analysis of an imported trajectory, what DENSE's [-i | --data-import]
+   flag was meant to do (main.cpp:160-175 with CSV_Streamed_Simulation,
+   io/csvr_sim.cpp:7-96, which never worked: its age_by calls itself): the
+   set's analyses, as created, see `num_samples` sampled states taken from
+   `samples` ([num_samples][num_species][num_cells]; species no analysis
+   observes are not read) instead of simulated ones, at the ages
+   time_start, time_start + analysis_interval, ... (each the previous plus
+   the interval, as age_by accumulates them), and the oscillation analyses
+   are then finalized; the results are read as after a run.  Call it on an
+   engine fresh from dense_engine_create or dense_engine_reset; it returns
+   when the analyses are done. */
+DENSE_API int dense_engine_analyze_samples(dense_engine* e, int set, const double* samples, int num_samples,
+                                           double time_start);
+
+/* Checkpoint and resume (no counterpart in DENSE, whose only record of a
+   run is its trajectory export).  A batch's whole mutable run state --
+   per-set progress and status, lag-0 state (and FP32 Kahan terms),
+   history rings and analysis state -- is copied into a caller buffer of
+   dense_engine_checkpoint_size bytes (a header that identifies the batch's
+   layout, then the four device blocks), after the engine's work so far
+   has finished.  dense_engine_restore puts such a snapshot back into an
+   engine created from the same inputs (the same sets, analyses, step
+   size, interval and precision, in this process or another one), which
+   then continues exactly where the checkpointed engine was: the rest of
+   the run gives the same results bit for bit as an uninterrupted one.  A
+   buffer too small, or a snapshot of a batch with another layout, returns
+   DENSE_ERR_INVALID and leaves the engine unchanged. */
+DENSE_API int dense_engine_checkpoint_size(dense_engine* e, int64_t* bytes);
+DENSE_API int dense_engine_checkpoint(dense_engine* e, void* buf, int64_t bytes);
+DENSE_API int dense_engine_restore(dense_engine* e, const void* buf, int64_t bytes);
 
 /* Per-set status words (DENSE_SET_* bits), [num_sets]: the drop that
    run_simulation makes when an analysis throws Bad_Simulation_Error

@@ -533,34 +533,62 @@ void oracle_steps(void* h, long n) {
 //   simulation, then (int)(interval / dt) steps and age += interval;
 //   at the end every oscillation analysis is finalized.
 // Returns the number of chunks run before the set was dropped (or all).
+// One round of analysis callbacks at the current age (run_simulation.hpp:
+// 131-136): each analysis samples the state if time-start <= age <
+// time-end; false when a concentration check failed.
+static bool callbacks(Sim* s) {
+  bool bad = false;
+  for (int key : s->order) {
+    int kind = key / 65536, idx = key % 65536;
+    if (kind == 0) {
+      Basic& b = s->basics[idx];
+      b.time = s->age;
+      if (b.time < b.t0 || b.time >= b.t1) continue;
+      basic_update(*s, b);
+    } else if (kind == 1) {
+      Oscil& o = s->oscils[idx];
+      o.time = s->age;
+      if (o.time < o.t0 || o.time >= o.t1) continue;
+      oscil_update(*s, o);
+    } else {
+      Check& ck = s->checks[idx];
+      ck.time = s->age;
+      if (ck.time < ck.t0 || ck.time >= ck.t1) continue;
+      if (!check_update(*s, ck)) bad = true;
+    }
+  }
+  return !bad;
+}
+
 long oracle_run(void* h, double duration, double interval) {
   Sim* s = static_cast<Sim*>(h);
   double chunks = duration / interval;
   long a = 0;
   for (a = 0; a < chunks; a++) {
-    bool bad = false;
-    for (int key : s->order) {
-      int kind = key / 65536, idx = key % 65536;
-      if (kind == 0) {
-        Basic& b = s->basics[idx];
-        b.time = s->age;
-        if (b.time < b.t0 || b.time >= b.t1) continue;
-        basic_update(*s, b);
-      } else if (kind == 1) {
-        Oscil& o = s->oscils[idx];
-        o.time = s->age;
-        if (o.time < o.t0 || o.time >= o.t1) continue;
-        oscil_update(*s, o);
-      } else {
-        Check& ck = s->checks[idx];
-        ck.time = s->age;
-        if (ck.time < ck.t0 || ck.time >= ck.t1) continue;
-        if (!check_update(*s, ck)) bad = true;
-      }
-    }
-    if (bad) { s->status |= ST_DROPPED; return a; }
+    if (!callbacks(s)) { s->status |= ST_DROPPED; return a; }
     int steps = static_cast<int>(interval / s->dt);
     for (int i = 0; i < steps; ++i) step(*s);
+    s->age += interval;
+  }
+  for (auto& o : s->oscils) oscil_finalize(o);
+  return a;
+}
+
+// The analyses over imported samples [k][NS][cells] instead of simulated
+// states (what DENSE's --data-import means to do, main.cpp:160-175): sample
+// a is written into the current rows, the analyses are called back at age
+// t0 + a intervals (accumulated), a failed check stops the run; the
+// oscillations are finalized at the end.  Returns the samples analysed.
+long oracle_replay(void* h, const double* samples, long k, double t0, double interval) {
+  Sim* s = static_cast<Sim*>(h);
+  s->age += t0;
+  long a = 0;
+  for (a = 0; a < k; a++) {
+    for (int sp = 0; sp < NS; ++sp) {
+      double* row = s->row_ptr(sp, 0);
+      for (int c = 0; c < s->cells; ++c) row[c] = samples[(static_cast<size_t>(a) * NS + sp) * s->cells + c];
+    }
+    if (!callbacks(s)) { s->status |= ST_DROPPED; return a; }
     s->age += interval;
   }
   for (auto& o : s->oscils) oscil_finalize(o);

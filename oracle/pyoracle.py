@@ -53,6 +53,8 @@ class OracleLib:
         lib.oracle_add_conccheck.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
                                              C.c_double, C.c_double, C.c_double]
         lib.oracle_steps.argtypes = [C.c_void_p, C.c_long]
+        lib.oracle_replay.restype = C.c_long
+        lib.oracle_replay.argtypes = [C.c_void_p, _D, C.c_long, C.c_double, C.c_double]
         lib.oracle_run.restype = C.c_long
         lib.oracle_run.argtypes = [C.c_void_p, C.c_double, C.c_double]
         lib.oracle_status.argtypes = [C.c_void_p]
@@ -133,6 +135,11 @@ class OracleSim:
 
     def steps(self, n):
         self.L.lib.oracle_steps(self.h, int(n))
+
+    def replay(self, samples, time_start, interval):
+        """The analyses over imported samples [k][species][cells]."""
+        x = np.ascontiguousarray(samples, np.float64)
+        return self.L.lib.oracle_replay(self.h, _dp(x), x.shape[0], float(time_start), float(interval))
 
     def run(self, duration, interval):
         return self.L.lib.oracle_run(self.h, float(duration), float(interval))

@@ -251,6 +251,43 @@ long oracle_run(void* p, double duration, double interval) {
   return a;
 }
 
+// DENSE's analyses over imported samples [k][NS][cells] (what its
+// --data-import means to do, main.cpp:160-175; its CSV_Streamed_Simulation
+// never worked, io/csvr_sim.cpp:87-96 calls itself): sample a is written
+// into DENSE's current rows (what get_concentration reads), the analyses
+// are called back as in oracle_run, and the age advances by the interval
+// through Simulation::age_by without stepping.  Returns the samples
+// analysed.
+long oracle_replay(void* p, const double* samples, long k, double t0, double interval) {
+  Harness* h = static_cast<Harness*>(p);
+  using D = std::chrono::duration<Real, std::chrono::minutes::period>;
+  Quiet q(h->sink);
+  h->sim->dense::Simulation::age_by(D(t0));
+  long a = 0;
+  for (a = 0; a < k; a++) {
+    for (int sp = 0; sp < NUM_SPECIES; ++sp) {
+      Real* row = h->sim->_baby_cl.row_at(sp, 0);
+      for (int c = 0; c < h->cells; ++c) row[c] = samples[(static_cast<size_t>(a) * NUM_SPECIES + sp) * h->cells + c];
+    }
+    bool bad = false;
+    for (auto& e : h->analyses) {
+      try {
+        e.a->when_updated_by(*h->sim, h->sink);
+      } catch (dense::Bad_Simulation_Error<Sim>&) {
+        bad = true;
+      }
+    }
+    if (bad) {
+      h->status |= 1;
+      return a;
+    }
+    h->sim->dense::Simulation::age_by(D(interval));
+    h->sink.str("");
+  }
+  for (auto& e : h->analyses) if (e.kind == 1) e.a->finalize();
+  return a;
+}
+
 int oracle_status(void* p) { return static_cast<Harness*>(p)->status; }
 double oracle_age(void* p) { return static_cast<Harness*>(p)->sim->age().count(); }
 

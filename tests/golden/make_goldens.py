@@ -100,6 +100,11 @@ CLI_CASES = {
     "turing_graphml_export": ("turing",
                               "-p {in}/turing_param_sets.csv -f {in}/organic2.graphml -t 4 -u 0.5 -s 0.01 "
                               "-d {in}/turing_init_conc.csv -e traj.csv -v", ["traj.csv"]),
+    # a trajectory export with its time column and species in non-id order:
+    # also the input of the -i (imported trajectory) cases below
+    "her_traj_export_v": ("her_model_2014",
+                          "-p {in}/her_param_sets.csv -c 12 -w 4 -t 30 -u 0.1 -s 0.01 -e traj.csv -v 1 "
+                          "-o \"ph1, mh1, md\"", ["traj.csv"]),
     "her_edge_list_export": ("her_model_2014",
                              "-p {in}/her_param_sets.csv -f {in}/cell_adj.g -t 30 -u 1 -s 0.01 -e traj.csv "
                              "-o \"mh1, ph1\"", ["traj.csv"]),
@@ -224,15 +229,100 @@ def run_ref(name):
     print("ref_%s.npz" % name, len(out), "arrays")
 
 
+# Analysis of imported trajectories (simulation -i): the trajectory file,
+# its analyses (analyses.xml text for the command, dicts for the harness),
+# -t and -u.  Fixture ref_<name>.npz: DENSE's own BasicAnalysis and
+# OscillationAnalysis over the file's samples (oracle_replay of the harness).
+IMPORT_CASES = {
+    "her_import_dense_export": dict(
+        file="cli/her_traj_export_v/traj.csv", minutes=30.0, interval=0.1,
+        analyses=[dict(kind="basic", species=["ph1", "mh1", "md"], cells=(0, 12), t=(0.0, 1e9)),
+                  dict(kind="oscillation", species=["mh1", "ph1"], cells=(0, 12), t=(0.0, 1e9), win=2.0, intvl=0.1)]),
+    "her_import_waves": dict(
+        file="inputs/her_traj_waves.csv", minutes=20.0, interval=0.1,
+        analyses=[dict(kind="basic", species=["mh1", "pd"], cells=(0, 7), t=(6.0, 1e9)),
+                  dict(kind="oscillation", species=["mh1"], cells=(0, 7), t=(5.0, 1e9), win=3.0, intvl=0.1)]),
+}
+
+
+def write_waves_trajectory():
+    """A seeded synthetic trajectory export (no DENSE run behind it): 10
+    cells of which 0-6 are exported, pd and mh1 columns in that order, time
+    starting at 5 min, 200 samples 0.1 min apart of waves whose period,
+    phase and amplitude differ per cell, written with every digit."""
+    import math
+    from dense_b200 import workloads
+    names = workloads.templates()["her_model_2014"]["species"]
+    rng = np.random.Generator(np.random.PCG64(51))
+    per = rng.uniform(1.5, 4.0, size=(2, 7))
+    ph = rng.uniform(0.0, 2 * math.pi, size=(2, 7))
+    amp = rng.uniform(1.0, 8.0, size=(2, 7))
+    cols = ["pd", "mh1"]
+    flags = ["1" if n in cols else "0" for n in names]
+    lines = ["", "# exported trajectory (synthetic)", "cell-total, time-start, time-col, cell-start, cell-end, "
+             "specie-option,", "10,5,0,0,7," + ",".join(flags) + ",", "", ",".join(cols) + ","]
+    for k in range(200):
+        t = 5.0 + 0.1 * k
+        for c in range(7):
+            v = [20.0 + amp[j, c] * math.sin(2 * math.pi * t / per[j, c] + ph[j, c]) + 0.01 * rng.normal()
+                 for j in range(2)]
+            lines.append(",".join(repr(float(x)) for x in v) + ",")
+        lines.append("")
+    with open(os.path.join(HERE, "inputs", "her_traj_waves.csv"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def import_samples(name):
+    """(header, samples [k][species][cells], species names) of an import case."""
+    from dense_b200 import csvio, workloads
+    names = workloads.templates()["her_model_2014"]["species"]
+    case = IMPORT_CASES[name]
+    head, x = csvio.read_trajectory(open(os.path.join(HERE, case["file"])).read(), names)
+    k = min(int(np.ceil(case["minutes"] / case["interval"])), x.shape[0])
+    return head, x[:k], names
+
+
+def run_import(name):
+    from oracle.pyoracle import load_ref
+    case = IMPORT_CASES[name]
+    head, x, names = import_samples(name)
+    R = load_ref("her_model_2014")
+    cells = head["cell_total"]
+    nprm = R.num_params
+    sim = R.create(np.zeros(cells + 1, np.int32), np.zeros(1, np.int32), np.zeros((cells, nprm)), np.zeros(nprm),
+                   None, case["interval"])
+    for a in case["analyses"]:
+        sp = [names.index(n) for n in a["species"]]
+        if a["kind"] == "basic":
+            sim.add_basic(sp, a["cells"][0], a["cells"][1], a["t"][0], a["t"][1])
+        else:
+            sim.add_oscillation(sp, a["cells"][0], a["cells"][1], a["t"][0], a["t"][1], a["win"], a["intvl"])
+    out = {"chunks": sim.replay(x, head["time_start"], case["interval"]), "status": np.int32(sim.status())}
+    for i, a in enumerate(case["analyses"]):
+        if a["kind"] == "basic":
+            b = sim.basic(i)
+            for k in ("mins", "sums", "maxs", "samples", "time", "cell_mins", "cell_sums", "cell_maxs"):
+                out["a%d_%s" % (i, k)] = np.asarray(b[k])
+        else:
+            o = sim.oscillation(i)
+            for k in ("amps", "pers", "avg_peak", "ncrit", "samples", "time"):
+                out["a%d_%s" % (i, k)] = np.asarray(o[k])
+    np.savez_compressed(os.path.join(HERE, "ref_%s.npz" % name), **out)
+    print("ref_%s.npz" % name, len(out), "arrays")
+
+
 if __name__ == "__main__":
     # no arguments: the CTest files, the command-line cases and every small
     # case; names (from CASES or FULL_CASES) regenerate just those fixtures
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:
-            run_ref(name)
+            run_import(name) if name in IMPORT_CASES else run_ref(name)
     else:
         copy_ctest()
         copy_inputs()
+        write_waves_trajectory()
         run_cli_cases()
         for name in CASES:
             run_ref(name)
+        for name in IMPORT_CASES:
+            run_import(name)

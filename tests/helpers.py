@@ -48,12 +48,14 @@ def run_oracle(lib, name):
     return out
 
 
-def run_engine(name, precision=0, graph=False, chunks_per_call=-1):
-    """The case through the CUDA engine (one batch holding all its sets)."""
+def run_engine(name, precision=0, graph=False, chunks_per_call=-1, schedule=0):
+    """The case through the CUDA engine (one batch holding all its sets,
+    every set with the schedule hint `schedule`)."""
     from dense_b200.engine import Analysis, Batch, ParameterSet
     case = build_case(name)
     sets = [ParameterSet(ps["off"], ps["ids"], ps["set_params"], cell_params=ps["cell_params"],
-                         init_conc=ps["init_conc"], perturb=ps.get("perturb"), duration=ps["duration"])
+                         init_conc=ps["init_conc"], perturb=ps.get("perturb"), duration=ps["duration"],
+                         schedule=schedule)
             for ps in case["sets"]]
     an = []
     for a in case["analyses"]:

@@ -79,7 +79,7 @@ def test_unknown_precision():
 
 
 @pytest.mark.parametrize("schedule,mem_block,msg", [
-    (5, 0, "schedule hint"), (-1, 0, "schedule hint"), (1, 48, "mem_block"), (1, 512, "mem_block"),
+    (7, 0, "schedule hint"), (-1, 0, "schedule hint"), (1, 48, "mem_block"), (1, 512, "mem_block"),
     (1, 16, "mem_block"),
 ])
 def test_bad_schedule_hints(schedule, mem_block, msg):
@@ -162,6 +162,8 @@ def test_every_entry_point_refuses_null_arguments():
         "dense_engine_copy_trajectory": (None, 0, None, 0, None, None),
         "dense_engine_trajectory_capacity": (None, 0, None), "dense_engine_info": (None, None, None, None),
         "dense_engine_ring_info": (None, 0, None, None), "dense_graph_launch": (None, None),
+        "dense_engine_checkpoint_size": (None, None), "dense_engine_checkpoint": (None, None, 0),
+        "dense_engine_restore": (None, None, 0),
         "dense_graph_capture": (0, None, None, 0, 0, None), "dense_engine_create": (None, 0, None, None),
         "dense_engine_plan": (None, 0, None, None, None, None), "dense_model_get_info": (None,),
     }

@@ -39,7 +39,6 @@ def _run(cli, args, cwd):
     (["-p", PARAMS, "-t", "10", "-s", "0.01", "-u", "0.1"], "cell-graph"),
     (["-c", "10"], "useless state"),
     (["-p", PARAMS, "-g", "grad.csv"] + BASE, "--gradients] is not supported"),
-    (["-p", PARAMS, "-i", "data.csv"] + BASE, "--data-import] (analysis of an imported trajectory) is not"),
 ])
 def test_bad_invocations_exit_1_with_a_message(cli, tmp_path, args, msg):
     rc, out = _run(cli, args, tmp_path)

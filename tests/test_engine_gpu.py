@@ -28,6 +28,18 @@ def test_fp64_bitwise_vs_dense_fixture(name):
     assert mismatches(want, got) == []
 
 
+@pytest.mark.parametrize("name", ["her_test", "her_pert", "her_sets", "her_delays", "her_cfg1_full", "bz",
+                                  "delay_reaction"])
+def test_shared_rows_and_register_kernels_both_match_dense(name):
+    """Sets without in-order reads run in the register kernel, or on request
+    in the wave kernel with their history rows in shared memory: both give
+    DENSE's outputs bit for bit."""
+    want = load_fixture(name)
+    for schedule in (E.SCHEDULE_SHARED_ROWS, E.SCHEDULE_REGISTER):
+        got = run_engine(name, schedule=schedule)
+        assert mismatches(want, got) == [], schedule
+
+
 @pytest.mark.parametrize("name", ["her_pert", "her_sets"])
 def test_fp64_bitwise_vs_oracle(name):
     from oracle.pyoracle import load_oracle
@@ -276,3 +288,48 @@ def test_fp32_kahan_turing_close_to_fp64():
     for a, f in zip(res[E.FP64] + basic[E.FP64], res[E.FP32_KAHAN] + basic[E.FP32_KAHAN]):
         rel = np.max(np.abs(a - f) / np.maximum(np.abs(a), 1e-3))
         assert rel < 1e-4, rel
+
+
+def test_checkpoint_and_resume_continue_bit_for_bit():
+    """A checkpoint taken mid-run and restored -- into a new batch built from
+    the same inputs, or into the same batch after it ran on -- continues to
+    the same final state and analysis outputs as the uninterrupted run; a
+    snapshot of another layout or a truncated one is refused."""
+    full = run_engine("her_sets")
+    from tests.golden.cases import build_case
+    case = build_case("her_sets")
+
+    def batch():
+        sets = [E.ParameterSet(ps["off"], ps["ids"], ps["set_params"], duration=ps["duration"])
+                for ps in case["sets"]]
+        an = [E.Analysis.basic(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1])
+              if a["kind"] == "basic" else
+              E.Analysis.oscillation(a["species"], a["cells"][0], a["cells"][1], a["t"][0], a["t"][1], a["win"],
+                                     a["intvl"]) for a in case["analyses"]]
+        return E.Batch(case["model"], sets, case["dt"], case["interval"], an)
+
+    a = batch()
+    a.run(517)
+    snap = a.checkpoint()
+    a.run(-1)
+    b = batch()
+    b.restore(snap)
+    b.run(-1)
+    a.restore(snap)   # back in time on the same engine
+    a.run(-1)
+    for x in (a, b):
+        for s in range(len(case["sets"])):
+            assert np.array_equal(x.state(s), full["state_%d" % s])
+            o = x.oscillation(1, s)
+            assert np.array_equal(o["pers"], full["a1_pers_%d" % s], equal_nan=True)
+            assert np.array_equal(o["amps"], full["a1_amps_%d" % s], equal_nan=True)
+            r = x.basic(0, s)
+            assert np.array_equal(r["sums"], full["a0_sums_%d" % s])
+    with pytest.raises(E.DenseError):
+        b.restore(snap[:100])
+    from dense_b200 import workloads
+    other = _her_batch([workloads.template_params()])
+    with pytest.raises(E.DenseError):
+        other.restore(snap)
+    for x in (a, b, other):
+        x.close()
