@@ -59,6 +59,7 @@ enum OscField : int {
   kOscTm2, kOscTm1,                 // times of critical points ncrit-3 and ncrit-2
   kOscPeakSum, kOscTroughSum, kOscNumPeaks, kOscNumTroughs, kOscCycleSum, kOscCycles,
   kOscAmp, kOscPer, kOscAvgPeak,    // results, written by finalize
+  kOscSame,                         // length of the run of equal values that ends at the newest one
   kOscFields
 };
 

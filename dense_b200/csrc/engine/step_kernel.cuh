@@ -277,18 +277,22 @@ __device__ __forceinline__ void osc_add_crit(const OscRef& o, double t, double c
 // is processed; loaded and stored as one batch of independent accesses.
 struct OscQueue {
   long start, end, current, live;
+  long same;  // the newest `same` values are equal (so the window is flat when same >= live)
   __device__ __forceinline__ void load(const OscRef& o) {
     const double s0 = o.f(kOscStart), e0 = o.f(kOscEnd), c0 = o.f(kOscCurrent), l0 = o.f(kOscLive);
+    const double m0 = o.f(kOscSame);
     start = static_cast<long>(s0);
     end = static_cast<long>(e0);
     current = static_cast<long>(c0);
     live = static_cast<long>(l0);
+    same = static_cast<long>(m0);
   }
   __device__ __forceinline__ void store(const OscRef& o) const {
     o.f(kOscStart) = static_cast<double>(start);
     o.f(kOscEnd) = static_cast<double>(end);
     o.f(kOscCurrent) = static_cast<double>(current);
     o.f(kOscLive) = static_cast<double>(live);
+    o.f(kOscSame) = static_cast<double>(same);
   }
   // Queue::dequeue (the value leaves DENSE's multiset too)
   __device__ __forceinline__ void dequeue(int w) {
@@ -307,7 +311,10 @@ struct OscQueue {
 // lies above it and some lies below, a trough when none lies below.  The
 // window is scanned from both ends inwards, four values from each end at a
 // time, and the scan stops as soon as values above and below have both been
-// seen, so only an extreme middle value costs a whole pass.  A middle index
+// seen, so only an extreme middle value costs a whole pass -- and a flat
+// window (every live value equal, known from the run of equal newest
+// values, and equal to the middle value) none: the middle value is then a
+// trough.  A middle index
 // of -1 (DENSE reads contents[-1]), an empty window or a NaN middle value
 // gives no critical point; NaN values in the window compare neither above
 // nor below (DENSE keeps them in a std::multiset, whose order NaN breaks).
@@ -317,6 +324,14 @@ __device__ __forceinline__ void osc_check(const OscRef& o, const OscQueue& q, co
   const double mid = win[static_cast<size_t>(q.current) * m];
   if (isnan(mid)) return;
   bool above = false, below = false;
+  if (q.same >= q.live && mid == win[static_cast<size_t>(q.end) * m]) {
+    // every live value equals the newest one, and so mid (a run of equal
+    // values holds no NaN)
+    double t = (samples - static_cast<double>(A.range_steps / 2)) * A.interval + A.t0;
+    t = (0.0 < t) ? t : 0.0;
+    osc_add_crit(o, t, mid, false);
+    return;
+  }
   long lo = q.start, hi = q.end;  // oldest and newest live slots
   long left = q.live;             // live values not yet looked at
   while (left > 0 && !(above && below)) {
@@ -370,6 +385,9 @@ __device__ __forceinline__ void osc_cell_update(double* st, const AnalysisDesc& 
     const double added = vals(A.slot[i], c);
     OscQueue q;
     q.load(o);
+    // the run of equal newest values (NaN equals nothing)
+    const double newest = q.live > 0 ? win[static_cast<size_t>(q.end) * m] : added;
+    q.same = (q.live > 0 && newest == added) ? q.same + 1 : (added == added ? 1 : 0);
     // Queue::enqueue; the multiset gains `added`
     q.end = (q.end == w - 1) ? 0 : q.end + 1;
     win[static_cast<size_t>(q.end) * m] = added;
