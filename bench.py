@@ -58,7 +58,7 @@ sys.path.insert(0, ROOT)
 #         terms (mul + add) and 14 Euler updates (mul + add) = 209.
 BYTES_PER_CELL_STEP = 304
 FLOPS_PER_CELL_STEP = 209
-DRAM_BYTES_PER_CELL_STEP = 17.7
+DRAM_BYTES_PER_CELL_STEP = 16.4
 
 METRIC = "cell-steps/s (FP64 plain)"
 
@@ -671,8 +671,8 @@ def main():
     achieved_gbs = BYTES_PER_CELL_STEP * per_launch_cell_steps / avg_launch_s / 1e9
     # DRAM traffic of one launch, scaled from an ncu capture of a smaller
     # launch of the same kernel and workload shape (296 sets x 200 cells x
-    # 1000 steps: dram__bytes_read.sum + dram__bytes_write.sum = 1.048 GB,
-    # 17.7 B per cell-step, cold caches); FP64 with Oscillation only
+    # 1000 steps: dram__bytes_read.sum + dram__bytes_write.sum = 0.973 GB,
+    # 16.4 B per cell-step, cold caches); FP64 with Oscillation only
     traffic = None
     if precision == E.FP64 and analyses:
         traffic = DRAM_BYTES_PER_CELL_STEP * per_launch_cell_steps
