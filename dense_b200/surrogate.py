@@ -58,12 +58,16 @@ def lib():
         L = C.CDLL(build())
         vp, i, f, i64 = C.c_void_p, C.c_int, C.c_float, C.c_int64
         L.dense_mlp_gemm.argtypes = [vp, i, vp, i, vp, i, i, i, i, i, vp, vp, i, vp, vp]
+        L.dense_mlp_gemm_ws.argtypes = [vp, i, vp, i, vp, i, i, i, i, i, vp, vp, i, vp, vp, C.c_size_t, vp]
         L.dense_mlp_transpose_bf16.argtypes = [vp, i, i, i, vp, i, vp]
         L.dense_mlp_cast_bf16.argtypes = [vp, i, i, vp, i, vp]
         L.dense_mlp_gelu_backward.argtypes = [vp, vp, i64, vp, vp, vp]
         L.dense_mlp_mse.argtypes = [vp, i, vp, vp, i, i, f, vp, vp, vp, vp]
         L.dense_mlp_colsum.argtypes = [vp, i, i, vp, vp]
         L.dense_mlp_adam.argtypes = [vp, vp, vp, vp, i64, f, f, f, f, i, vp]
+        L.dense_mlp_adam_dev.argtypes = [vp, vp, vp, vp, i64, vp, vp]
+        L.dense_mlp_mse_dev.argtypes = [vp, i, vp, vp, i, i, vp, vp, vp, vp, vp]
+        L.dense_mlp_gather.argtypes = [vp, i, i, vp, vp, i, vp, i, i, vp, i, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -73,7 +77,12 @@ def _p(t):
 
 
 class Kernels:
-    """Thin launchers over the C ABI for torch CUDA tensors on one stream."""
+    """Thin launchers over the C ABI for torch CUDA tensors on one stream.
+
+    The GEMM's split-K workspace (FP32 partials) belongs to this object:
+    its launches must stay on one stream."""
+
+    WS_BYTES = 32 << 20
 
     def __init__(self, device=0):
         import torch
@@ -82,6 +91,7 @@ class Kernels:
         self.dev = torch.device("cuda", device)
         self.stream = torch.cuda.current_stream(self.dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.ws = torch.empty(self.WS_BYTES // 4, dtype=torch.float32, device=self.dev)
 
     def _s(self):
         return C.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
@@ -90,8 +100,9 @@ class Kernels:
         """D[M][N] = A[M][K] . B[N][K]^T (BF16 in, FP32 out)."""
         M, K = A.shape
         N = B.shape[0]
-        rc = self.L.dense_mlp_gemm(_p(A), A.stride(0), _p(B), B.stride(0), _p(D), D.stride(0), M, N, K, epilogue,
-                                   _p(bias), _p(H), H.stride(0) if H is not None else 0, _p(self.err), self._s())
+        rc = self.L.dense_mlp_gemm_ws(_p(A), A.stride(0), _p(B), B.stride(0), _p(D), D.stride(0), M, N, K, epilogue,
+                                      _p(bias), _p(H), H.stride(0) if H is not None else 0, _p(self.err),
+                                      _p(self.ws), self.WS_BYTES, self._s())
         if rc:
             raise RuntimeError("dense_mlp_gemm rejected M=%d N=%d K=%d (rc %d)" % (M, N, K, rc))
 
@@ -111,6 +122,25 @@ class Kernels:
         inv = 1.0 / max(1.0, float(mask.sum().item()))
         assert self.L.dense_mlp_mse(_p(Y), Y.stride(0), _p(T), _p(mask), rows, nout, inv, _p(dY), _p(dYb),
                                     _p(loss), self._s()) == 0
+
+    def mse_dev(self, Y, T, mask, inv_count, dY, dYb, loss):
+        """mse with the 1 / count scale in a one-element device tensor."""
+        rows, nout = T.shape
+        assert self.L.dense_mlp_mse_dev(_p(Y), Y.stride(0), _p(T), _p(mask), rows, nout, _p(inv_count), _p(dY),
+                                        _p(dYb), _p(loss), self._s()) == 0
+
+    def gather(self, X, T, mask, idx, Xb, Tb, Mb):
+        """One batch from a device-resident training set: rows idx of X
+        (float [n][n_in]) to BF16 Xb [Bp][in_pad] (zero padded), of T and
+        mask to Tb and Mb [Bp][n_out]; rows past len(idx) are zeros."""
+        n, n_in = X.shape
+        Bp, in_pad = Xb.shape
+        assert self.L.dense_mlp_gather(_p(X), n, n_in, _p(T), _p(mask), T.shape[1], _p(idx), idx.shape[0], Bp,
+                                       _p(Xb), in_pad, _p(Tb), _p(Mb), self._s()) == 0
+
+    def adam_dev(self, w, g, m, v, hyper):
+        """adam with {lr, b1, b2, eps, 1 - b1^t, 1 - b2^t} in device memory."""
+        assert self.L.dense_mlp_adam_dev(_p(w), _p(g), _p(m), _p(v), w.numel(), _p(hyper), self._s()) == 0
 
     def colsum(self, dZ, db):
         r, c = dZ.shape
@@ -246,6 +276,14 @@ class MLP:
         dY = self._buf("dY", (Bp, OUT_PAD))
         dYb = self._buf("dYb", (Bp, OUT_PAD), bf)
         self.k.mse(Y, Tt, Mt, dY, dYb, loss)
+        dW, db = self._backward(dY, dYb, Bp)
+        self.k.check()
+        return float(loss.item()), dW, db
+
+    def _backward(self, dY, dYb, Bp):
+        """Weight and bias gradients from the output gradient dY (FP32 and
+        BF16 copies) of the last forward pass over Bp rows."""
+        bf = self.torch.bfloat16
         dW = [None] * 4
         db = [None] * 4
         dZ, dZb = dY, dYb
@@ -269,8 +307,112 @@ class MLP:
             ndZb = self._buf("dZb%d" % (i - 1), (Bp, HIDDEN), bf)
             self.k.gelu_backward(dH, self.Z[i - 1], ndZ, ndZb)
             dZ, dZb = ndZ, ndZb
-        self.k.check()
-        return float(loss.item()), dW, db
+        return dW, db
+
+    def _train_graphs(self, data, batch, steps):
+        """CUDA graphs of training on the device-resident training set
+        `data` = (X, T, mask), `steps` steps of `batch` rows per epoch.
+        Per epoch the host writes the epoch's row indices ("idx", steps x
+        batch) and per-step scalars ("hyper", steps x {lr, b1, b2, eps,
+        1 - b1^t, 1 - b2^t, 1 / count}) into static device buffers.  One
+        process: one graph replays the whole epoch (per step: batch gather,
+        weight casts, forward, loss, backward, Adam).  Data-parallel: per
+        step a gradient graph and an update graph, with the gradient
+        all-reduce between them.  The graphs hold the addresses of this
+        object's work buffers: they serve one fit call only (no other pass
+        may resize a buffer meanwhile)."""
+        torch = self.torch
+        Bp = (batch + 127) // 128 * 128
+        bf = torch.bfloat16
+        g = {"Bp": Bp}
+        g["idx"] = torch.zeros(steps * batch, dtype=torch.int32, device=self.dev)
+        g["hyper"] = torch.zeros((steps, 8), device=self.dev)
+        g["loss"] = torch.zeros(1, device=self.dev)
+        Xd, Td, Md = data
+
+        def grads(j):
+            self._cast_weights()
+            Xb = self._buf("Xb", (Bp, IN_PAD), bf)
+            Tb = self._buf("Tb", (Bp, self.n_out))
+            Mb = self._buf("Mb", (Bp, self.n_out))
+            self.k.gather(Xd, Td, Md, g["idx"][j * batch:(j + 1) * batch], Xb, Tb, Mb)
+            Y = self.forward(Xb)
+            dY = self._buf("dY", (Bp, OUT_PAD))
+            dYb = self._buf("dYb", (Bp, OUT_PAD), bf)
+            self.k.mse_dev(Y, Tb, Mb, g["hyper"][j, 6:7], dY, dYb, g["loss"])
+            g["dW"], g["db"] = self._backward(dY, dYb, Bp)
+
+        def update(j):
+            hyper = g["hyper"][j]
+            for i in range(4):
+                self.k.adam_dev(self.W[i], g["dW"][i], self.mW[i], self.vW[i], hyper)
+                self.k.adam_dev(self.b[i], g["db"][i], self.mb[i], self.vb[i], hyper)
+
+        side = torch.cuda.Stream(self.dev)
+        side.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(side):
+            grads(0)  # allocates every buffer before capture; changes no weight
+        torch.cuda.current_stream(self.dev).wait_stream(side)
+        torch.cuda.synchronize(self.dev)
+        if self.group is None:
+            g["epoch"] = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g["epoch"]):
+                for j in range(steps):
+                    grads(j)
+                    update(j)
+        else:
+            g["grads"], g["update"] = [], []
+            for j in range(steps):
+                gg, gu = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+                with torch.cuda.graph(gg):
+                    grads(j)
+                with torch.cuda.graph(gu):
+                    update(j)
+                g["grads"].append(gg)
+                g["update"].append(gu)
+        return g
+
+    def _fit_captured(self, X, T, mask, n, epochs, batch, rng, log, cosine, b1=0.9, b2=0.999, eps=1e-8):
+        torch = self.torch
+        steps = n // batch
+        hist = []
+        if steps == 0:
+            return [0.0] * epochs
+        Xd = torch.as_tensor(np.ascontiguousarray(X, dtype=np.float32), device=self.dev)
+        Td = torch.as_tensor(np.ascontiguousarray(np.nan_to_num(T), dtype=np.float32), device=self.dev)
+        Md = torch.as_tensor(np.ascontiguousarray(mask, dtype=np.float32), device=self.dev)
+        g = self._train_graphs((Xd, Td, Md), batch, steps)
+        lr0 = self.lr
+        total = epochs * steps
+        for ep in range(epochs):
+            rows = rng.permutation(X.shape[0])[:n][:steps * batch]
+            counts = mask[rows].reshape(steps, batch, -1).sum(axis=(1, 2), dtype=np.float64)
+            hyp = np.zeros((steps, 8), np.float64)
+            for j in range(steps):
+                lr = lr0
+                if cosine:
+                    t = (ep * steps + j) / max(1, total - 1)
+                    lr = lr0 * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * t)))
+                step = self.steps + j + 1
+                hyp[j] = (lr, b1, b2, eps, 1.0 - b1 ** step, 1.0 - b2 ** step, 1.0 / max(1.0, counts[j]), 0.0)
+            g["idx"].copy_(torch.as_tensor(rows.astype(np.int32)))
+            g["hyper"].copy_(torch.as_tensor(hyp.astype(np.float32)))
+            g["loss"].zero_()
+            if self.group is None:
+                g["epoch"].replay()
+            else:
+                from .distributed import average_
+                for j in range(steps):
+                    g["grads"][j].replay()
+                    average_(g["dW"] + g["db"], self.group)
+                    g["update"][j].replay()
+            self.steps += steps
+            hist.append(float(g["loss"].item()) / steps)
+            self.k.check()
+            if log:
+                log("epoch %d loss %.5f" % (ep, hist[-1]))
+        del g
+        return hist
 
     def step(self, X, T, mask):
         loss, dW, db = self.gradients(X, T, mask)
@@ -283,9 +425,12 @@ class MLP:
             self.k.adam(self.b[i], db[i], self.mb[i], self.vb[i], self.lr, self.steps)
         return loss
 
-    def fit(self, X, T, mask, epochs=20, batch=4096, seed=0, log=None, cosine=True):
+    def fit(self, X, T, mask, epochs=20, batch=4096, seed=0, log=None, cosine=True, captured=True):
         """Minibatch Adam; with `cosine` the learning rate follows a cosine
-        from lr down to lr/100 over the run."""
+        from lr down to lr/100 over the run.  With `captured` (the default)
+        the training set is copied to the GPU once and every step replays
+        two CUDA graphs (gradient, update); otherwise each step is launched
+        from the host (`step`), with the same batches and schedule."""
         rng = np.random.Generator(np.random.PCG64(seed))
         n = X.shape[0]
         if self.group is not None:
@@ -294,6 +439,8 @@ class MLP:
             t = self.torch.tensor([n], device=self.dev)
             dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
             n = int(t.item())
+        if captured:
+            return self._fit_captured(X, T, mask, n, epochs, batch, rng, log, cosine)
         hist = []
         lr0 = self.lr
         per_epoch = max(1, n // batch)

@@ -30,6 +30,14 @@ def test_library_exports_every_declared_symbol(model):
         assert hasattr(lib, s), s
 
 
+def test_surrogate_library_exports_its_entry_points():
+    from dense_b200 import surrogate
+    lib = ctypes.CDLL(surrogate.build())
+    for name in ("dense_mlp_gemm", "dense_mlp_gemm_ws", "dense_mlp_transpose_bf16", "dense_mlp_cast_bf16",
+                 "dense_mlp_gelu_backward", "dense_mlp_mse", "dense_mlp_colsum", "dense_mlp_adam"):
+        assert hasattr(lib, name), name
+
+
 def test_model_info_matches_oracle():
     from dense_b200.engine import load
     from oracle.pyoracle import load_oracle

@@ -7,8 +7,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+# N not a multiple of 32 takes the one-tile-per-CTA kernels; the others the
+# persistent kernel: resident B (K <= 256), streamed B (K = 512), more row
+# tiles than SMs (both accumulators of a CTA in use), split K (few row
+# tiles, long K).
 @pytest.mark.parametrize("M,N,K", [(128, 256, 64), (256, 16, 64), (512, 128, 256), (256, 64, 4096),
-                                   (128, 48, 128), (384, 256, 256)])
+                                   (128, 48, 128), (384, 256, 256), (40960, 256, 64), (40960, 128, 256),
+                                   (20480, 256, 512), (256, 256, 4096), (128, 32, 8192), (1024, 64, 1024)])
 def test_umma_gemm_matches_fp32_product(M, N, K):
     import torch
     from dense_b200.surrogate import Kernels
@@ -22,6 +27,120 @@ def test_umma_gemm_matches_fp32_product(M, N, K):
     ref = A.float() @ B.float().T
     err = (D - ref).abs().max().item() / ref.abs().max().item()
     assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("M,N,K", [(40960, 256, 256), (256, 128, 2048)])
+def test_persistent_gemm_epilogues(M, N, K):
+    """Bias and bias+GELU through the persistent kernel's TMA-store
+    epilogue (first shape) and the split-K reduction (second), into
+    matrices whose leading dimension exceeds N."""
+    import torch
+    from dense_b200.surrogate import EPI_BIAS, EPI_BIAS_GELU, Kernels
+    k = Kernels()
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    Zw = torch.full((M, N + 64), float("nan"), device="cuda")
+    Hw = torch.zeros((M, N + 32), device="cuda", dtype=torch.bfloat16)
+    Z, H = Zw[:, :N], Hw[:, :N]
+    k.gemm(A, B, Z, EPI_BIAS_GELU, bias, H)
+    Y = torch.empty(M, N, device="cuda")
+    k.gemm(A, B, Y, EPI_BIAS, bias)
+    k.check()
+    ref = A.float() @ B.float().T + bias
+    scale = ref.abs().max().item()
+    assert (Z - ref).abs().max().item() < 1e-5 * scale
+    assert (Y - ref).abs().max().item() < 1e-5 * scale
+    assert torch.isnan(Zw[:, N:]).all(), "columns past N were written"
+    gelu = torch.nn.functional.gelu(ref)
+    assert (H.float() - gelu).abs().max().item() < 1e-2 * max(1.0, gelu.abs().max().item())
+    assert (Hw[:, N:] == 0).all()
+
+
+def test_split_k_is_deterministic():
+    """Split-K sums the partials in split order: repeated products are
+    bit-identical."""
+    import torch
+    from dense_b200.surrogate import Kernels
+    k = Kernels()
+    g = torch.Generator(device="cuda").manual_seed(11)
+    A = torch.randn(256, 4096, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(256, 4096, device="cuda", generator=g).to(torch.bfloat16)
+    outs = []
+    for _ in range(5):
+        D = torch.empty(256, 256, device="cuda")
+        k.gemm(A, B, D)
+        outs.append(D)
+    k.check()
+    for D in outs[1:]:
+        assert torch.equal(D, outs[0])
+
+
+@pytest.mark.parametrize("rows,cols", [(4096, 256), (4133, 200), (5, 64), (0, 32)])
+def test_column_sums(rows, cols):
+    """The bias gradient's column sums (cluster reduction over distributed
+    shared memory) against a float64 sum, and bit-identical on repeat."""
+    import torch
+    from dense_b200.surrogate import Kernels
+    k = Kernels()
+    g = torch.Generator(device="cuda").manual_seed(rows + cols)
+    Z = torch.randn(rows, cols, device="cuda", generator=g)
+    db = torch.full((cols,), float("nan"), device="cuda")
+    k.colsum(Z, db)
+    db2 = torch.empty_like(db)
+    k.colsum(Z, db2)
+    torch.cuda.synchronize()
+    ref = Z.double().sum(0)
+    assert (db.double() - ref).abs().max().item() <= 1e-5 * max(1.0, Z.abs().sum(0).max().item())
+    assert torch.equal(db, db2)
+
+
+def test_batch_gather_matches_numpy():
+    import torch
+    from dense_b200.surrogate import IN_PAD, Kernels
+    k = Kernels()
+    rng = np.random.Generator(np.random.PCG64(4))
+    X = rng.normal(size=(1000, 44)).astype(np.float32)
+    T = rng.normal(size=(1000, 5)).astype(np.float32)
+    M = (rng.uniform(size=(1000, 5)) > 0.3).astype(np.float32)
+    idx = rng.permutation(1000)[:300].astype(np.int32)
+    dev = torch.device("cuda")
+    Xb = torch.full((384, IN_PAD), 7.0, device=dev).to(torch.bfloat16)
+    Tb = torch.full((384, 5), 7.0, device=dev)
+    Mb = torch.full((384, 5), 7.0, device=dev)
+    k.gather(torch.tensor(X, device=dev), torch.tensor(T, device=dev), torch.tensor(M, device=dev),
+             torch.tensor(idx, device=dev), Xb, Tb, Mb)
+    torch.cuda.synchronize()
+    want = np.zeros((384, IN_PAD), np.float32)
+    want[:300, :44] = torch.tensor(X[idx]).to(torch.bfloat16).float().numpy()
+    assert np.array_equal(Xb.float().cpu().numpy(), want)
+    wt = np.zeros((384, 5), np.float32)
+    wt[:300] = T[idx]
+    wm = np.zeros((384, 5), np.float32)
+    wm[:300] = M[idx]
+    assert np.array_equal(Tb.cpu().numpy(), wt) and np.array_equal(Mb.cpu().numpy(), wm)
+
+
+def test_captured_training_follows_the_launched_steps():
+    """The graph-captured fit (device-resident data, two graphs per step)
+    takes the same batches, schedule and updates as the step-by-step path:
+    loss histories and weights agree to rounding."""
+    import torch
+    from dense_b200.surrogate import MLP
+    rng = np.random.Generator(np.random.PCG64(9))
+    X = rng.uniform(-1, 1, size=(6000, 10)).astype(np.float32)
+    T = np.stack([np.sin(2 * X[:, 0]), X[:, 1] * X[:, 2], np.cos(X[:, 3])], 1).astype(np.float32)
+    M = np.ones_like(T)
+    M[::7, 1] = 0
+    a, b = MLP(10, 3, seed=5), MLP(10, 3, seed=5)
+    ha = a.fit(X, T, M, epochs=3, batch=1024, seed=2, captured=True)
+    hb = b.fit(X, T, M, epochs=3, batch=1024, seed=2, captured=False)
+    assert a.steps == b.steps == 15
+    assert np.allclose(ha, hb, rtol=2e-3), (ha, hb)
+    for wa, wb in zip(a.W + a.b, b.W + b.b):
+        d = (wa - wb).norm().item() / max(wb.norm().item(), 1e-12)
+        assert d < 1e-3, d
 
 
 def test_umma_gemm_bias_gelu_epilogue():
