@@ -512,9 +512,10 @@ __device__ __forceinline__ bool analyses_sample(const StepArgs& a, double* anl, 
 
 // ---------------------------------------------------------------- kernel
 
-// kThreads / kMinBlocks: 224 threads with two resident CTAs per SM (a
-// 144-register budget) for sets of up to 224 cells, 256 threads with one
-// CTA per SM above that.
+// kThreads / kMinBlocks: 224 threads with two resident CTAs per SM for sets
+// of up to 224 cells (128 registers: the fourteen warps put four on the
+// busiest of the SM's four sub-partitions, whose register file holds
+// 16384), 256 threads with one CTA per SM above that.
 template <typename T, bool kKahan, int kThreads, int kMinBlocks, bool kUniform>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) dense_step_kernel(const StepArgs a, const int* set_list) {
   // dynamic shared memory: sampled state [NS][blockDim] (doubles, only with

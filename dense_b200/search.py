@@ -171,12 +171,12 @@ def targets(F):
 
 
 class Surrogate:
-    """The trained networks behind one predict(): every output (the 0/1
-    indicators included) is trained standardised (minus its mean over the
-    rows where it is defined, over its standard deviation there) and mapped
-    back on prediction; with
-    several networks (an ensemble of different initial weights and batch
-    orders) their outputs are averaged."""
+    """The trained networks behind one predict(): outputs trained
+    standardised (minus their mean over the rows where they are defined,
+    over their standard deviation there; mu 0 and sd 1 leave an output as
+    it is) are mapped back on prediction; with several networks (an
+    ensemble of different initial weights and batch orders) their outputs
+    are averaged."""
 
     def __init__(self, nets, mu, sd):
         self.nets, self.mu, self.sd = nets, np.asarray(mu, np.float32), np.asarray(sd, np.float32)
@@ -192,16 +192,19 @@ class Surrogate:
         return y * torch.as_tensor(self.sd, device=y.device) + torch.as_tensor(self.mu, device=y.device)
 
 
-def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, group=None, device=0, ensemble=1):
+def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, group=None, device=0, ensemble=1,
+                    standardize_indicators=False):
     """The MLP surrogate on (P, F): `ensemble` networks trained on
-    standardised targets; with a process group, data-parallel over the
-    ranks' shards (gradients averaged every step)."""
+    standardised regression targets (the 0/1 indicators too with
+    `standardize_indicators`, which weighs the rare acceptances up); with a
+    process group, data-parallel over the ranks' shards (gradients averaged
+    every step)."""
     from .surrogate import MLP
     X = encode(P)
     T, M = targets(F)
     mu = np.zeros(T.shape[1], np.float32)
     sd = np.ones(T.shape[1], np.float32)
-    for j in range(T.shape[1]):  # indicators too: rare acceptances then weigh as much as the rest
+    for j in range(T.shape[1] if standardize_indicators else 3):
         on = M[:, j] > 0
         if on.sum() > 1:
             mu[j] = float(T[on, j].mean())
@@ -226,11 +229,28 @@ def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, grou
     return Surrogate(nets, mu, sd)
 
 
+REGION_WEIGHT = 0.1   # weight of the predicted features' closeness to the acceptance region
+AMP_RAMP = 0.1        # log-amplitude width over which the amplitude term rises from 0 to 1
+
+
+def _region_terms(log_per, log_amp, p_osc, xp):
+    """Closeness of the predicted features to the acceptance region: minus
+    the period's distance from the target in tolerances, plus half a ramp
+    in log amplitude around AMP_MIN and half the oscillation indicator
+    (both clipped to [0, 1]); `xp` is numpy or torch."""
+    clip = (lambda x, lo, hi: xp.clip(x, lo, hi)) if xp is np else (lambda x, lo, hi: x.clamp(lo, hi))
+    per = xp.exp(clip(log_per, -10.0, 10.0))
+    amp_term = clip((log_amp - math.log(AMP_MIN)) / AMP_RAMP + 0.5, 0.0, 1.0)
+    return -xp.abs(per - TARGET_PERIOD) / PERIOD_TOL + 0.5 * amp_term + 0.5 * clip(p_osc, 0.0, 1.0)
+
+
 def predicted_score(pred):
-    """Higher is better: the predicted acceptance indicator, ties broken by
-    the predicted closeness to the period window."""
-    per = np.exp(np.clip(pred[:, 0], -10, 10))
-    return pred[:, 4] - 1e-3 * np.abs(per - TARGET_PERIOD) / PERIOD_TOL
+    """Higher is better: the predicted acceptance indicator plus
+    REGION_WEIGHT times the predicted features' closeness to the acceptance
+    region (the two together keep more of the candidates the FP64
+    simulation accepts than either alone)."""
+    pred = np.asarray(pred, np.float64)
+    return pred[:, 4] + REGION_WEIGHT * _region_terms(pred[:, 0], pred[:, 1], pred[:, 3], np)
 
 
 def score_candidates(net, P, chunk=1 << 20, spread=SPREAD):
@@ -248,8 +268,7 @@ def score_candidates(net, P, chunk=1 << 20, spread=SPREAD):
         x = torch.as_tensor(P[s:s + chunk], device=dev)[:, it]
         x = (torch.log(x / tt) / math.log(spread)).to(torch.float32)
         y = net.predict_device(x).to(torch.float64)
-        per = torch.exp(torch.clamp(y[:, 0], -10, 10))
-        out.append((y[:, 4] - 1e-3 * torch.abs(per - TARGET_PERIOD) / PERIOD_TOL).cpu().numpy())
+        out.append((y[:, 4] + REGION_WEIGHT * _region_terms(y[:, 0], y[:, 1], y[:, 3], torch)).cpu().numpy())
     return np.concatenate(out) if out else np.zeros(0)
 
 

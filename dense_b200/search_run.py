@@ -14,7 +14,8 @@
 Prints one JSON object.  Usage:
   python -m dense_b200.search_run [--train N] [--test N] [--candidates N]
       [--minutes M] [--resim-minutes R[,R2...]] [--cells C] [--epochs E]
-      [--generations G]
+      [--ensemble K] [--generations G] [--extrapolate N[,N2...]]
+      [--data-cache FILE]
 
 --minutes is the horizon of the training and held-out simulations (the
 features' window is 0-60 min, and the first 60 minutes of a run do not
@@ -44,17 +45,43 @@ import numpy as np
 from . import search as S
 
 
-def with_one_time_cost(res):
+def with_one_time_cost(res, candidates=None):
     """The screened search's rate charged with the surrogate's one-time cost
     (training simulations and training), crediting the sets the training
     simulations accepted, and its gain over plain search; None where the
-    run has no plain rate."""
+    run has no plain rate.  With `candidates` other than the run's, the
+    same figures for a search of that many candidates per trained network,
+    scaled from the run's measured parts: ranking, re-simulation and
+    accepted sets grow with the candidates, the one-time cost does not."""
     srch, data = res["search"], res["data"]
-    seconds = data["seconds"] + res["training_s"] + srch["inference_s"] + srch["resimulation_s"]
-    accepted = srch["accepted_screened"] + data["accepted_fraction"] * data["train_sets"]
+    scale = 1.0 if candidates is None else candidates / float(srch["candidates"])
+    seconds = data["seconds"] + res["training_s"] + scale * (srch["inference_s"] + srch["resimulation_s"])
+    accepted = scale * srch["accepted_screened"] + data["accepted_fraction"] * data["train_sets"]
     rate = accepted / seconds
     plain = srch["accepted_per_s_plain"]
-    return {"accepted_per_s": rate, "gain": rate / plain if plain > 0 else None, "seconds": seconds}
+    out = {"accepted_per_s": rate, "gain": rate / plain if plain > 0 else None, "seconds": seconds}
+    if candidates is not None:
+        out["candidates"] = candidates
+    return out
+
+
+def load_or_simulate(a, sim, log):
+    """Training and held-out candidates and their FP64 features; with
+    --data-cache, read from that file when it exists (the recorded
+    simulation seconds are the original run's) and written otherwise."""
+    import pickle
+    if a.data_cache and os.path.exists(a.data_cache):
+        with open(a.data_cache, "rb") as f:
+            return pickle.load(f), True
+    P_train = S.draw_candidates(a.train, a.seed)
+    F_train = S.simulate_features(P_train, log=log, **sim)
+    P_test = S.draw_candidates(a.test, a.seed + 1)
+    F_test = S.simulate_features(P_test, log=log, **sim)
+    data = (P_train, F_train, P_test, F_test)
+    if a.data_cache:
+        with open(a.data_cache, "wb") as f:
+            pickle.dump(data, f)
+    return data, False
 
 
 def main(argv=None):
@@ -70,9 +97,13 @@ def main(argv=None):
                     help="simulated minutes of the search's simulations, comma-separated")
     ap.add_argument("--cells", type=int, default=200)
     ap.add_argument("--epochs", type=int, default=150)
-    ap.add_argument("--ensemble", type=int, default=1, help="networks averaged by the surrogate")
+    ap.add_argument("--ensemble", type=int, default=4, help="networks averaged by the surrogate")
     ap.add_argument("--generations", type=int, default=3)
     ap.add_argument("--seed", type=int, default=100)
+    ap.add_argument("--extrapolate", default="58000000",
+                    help="candidate counts for the charged gain scaled from the measured run, comma-separated")
+    ap.add_argument("--data-cache", default=None,
+                    help="file holding the simulated training and held-out sets (read if present, else written)")
     a = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
@@ -80,10 +111,8 @@ def main(argv=None):
     sim = dict(minutes=a.minutes, cells=a.cells, width=4)
     res = {"config": vars(a)}
     t0 = time.perf_counter()
-    P_train = S.draw_candidates(a.train, a.seed)
-    F_train = S.simulate_features(P_train, log=log, **sim)
-    P_test = S.draw_candidates(a.test, a.seed + 1)
-    F_test = S.simulate_features(P_test, log=log, **sim)
+    (P_train, F_train, P_test, F_test), cached = load_or_simulate(a, sim, log)
+    res["data_cached"] = cached
     res["data"] = {"train_sets": a.train, "test_sets": a.test, "seconds": F_train["seconds"] + F_test["seconds"],
                    "cell_steps_per_s": (F_train["cell_steps"] + F_test["cell_steps"]) /
                                        (F_train["seconds"] + F_test["seconds"]),
@@ -100,6 +129,9 @@ def main(argv=None):
                               sim_kwargs=dict(sim, minutes=m), log=log)
         r["minutes"] = m
         r["with_one_time_cost"] = with_one_time_cost(dict(res, search=r))
+        if a.extrapolate:
+            r["with_one_time_cost_scaled"] = [with_one_time_cost(dict(res, search=r), int(float(c)))
+                                              for c in str(a.extrapolate).split(",")]
         res["search_by_horizon"]["%g" % m] = r
         if k == 0:
             res["search"] = r

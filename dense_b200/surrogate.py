@@ -497,12 +497,39 @@ def bench_gemm(rows=131072, reps=20, device=0):
     return out
 
 
+def bench_fit(rows=200000, epochs=3, batch=4096, n_in=44, n_out=5, device=0):
+    """Wall time per training step of MLP.fit on seeded random data, the
+    captured form (one CUDA graph per epoch) and the launched form; each
+    after a one-epoch warm-up on a slice, graph capture included."""
+    import time
+    import torch
+    rng = np.random.Generator(np.random.PCG64(0))
+    X = rng.uniform(-1, 1, size=(rows, n_in)).astype(np.float32)
+    T = rng.normal(size=(rows, n_out)).astype(np.float32)
+    M = np.ones((rows, n_out), np.float32)
+    out = []
+    for captured in (True, False):
+        net = MLP(n_in, n_out, seed=0, device=device)
+        net.fit(X[:8 * batch], T[:8 * batch], M[:8 * batch], epochs=1, batch=batch, captured=captured)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        net.fit(X, T, M, epochs=epochs, batch=batch, captured=captured)
+        torch.cuda.synchronize(device)
+        steps = epochs * (rows // batch)
+        out.append({"captured": captured, "rows": rows, "batch": batch, "epochs": epochs, "steps": steps,
+                    "ms_per_step": 1e3 * (time.perf_counter() - t0) / steps})
+    return out
+
+
 if __name__ == "__main__":
     import argparse
     import json
-    ap = argparse.ArgumentParser(description="time the surrogate's tensor-core GEMM")
+    ap = argparse.ArgumentParser(description="time the surrogate's tensor-core GEMM, or its training steps")
     ap.add_argument("--rows", type=int, default=131072)
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--fit", action="store_true", help="time MLP.fit steps instead (--rows training rows)")
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=4096)
     a = ap.parse_args()
-    for r in bench_gemm(a.rows, a.reps):
+    for r in (bench_fit(a.rows, a.epochs, a.batch) if a.fit else bench_gemm(a.rows, a.reps)):
         print(json.dumps(r))

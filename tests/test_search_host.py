@@ -104,9 +104,16 @@ def test_gain_with_one_time_cost():
     from dense_b200.search_run import with_one_time_cost
     res = {"data": {"seconds": 69.686775528, "train_sets": 200000, "accepted_fraction": 0.03212},
            "training_s": 49.90117416199999,
-           "search": {"inference_s": 0.4650351440000122, "resimulation_s": 31.993933156999987,
-                      "accepted_screened": 49294, "accepted_per_s_plain": 95.1213437156791}}
+           "search": {"candidates": 10000000, "inference_s": 0.4650351440000122,
+                      "resimulation_s": 31.993933156999987, "accepted_screened": 49294,
+                      "accepted_per_s_plain": 95.1213437156791}}
     r = with_one_time_cost(res)
     assert abs(r["accepted_per_s"] - 366.45) < 0.1 and abs(r["gain"] - 3.85) < 0.01
+    # scaled to 58M candidates: 5.8x the search parts, the same one-time cost
+    r58 = with_one_time_cost(res, 58000000)
+    want = (5.8 * 49294 + 0.03212 * 200000) / (69.686775528 + 49.90117416199999 + 5.8 * (0.4650351440000122 +
+                                                                                     31.993933156999987))
+    assert abs(r58["accepted_per_s"] - want) < 1e-9 and r58["candidates"] == 58000000
+    assert abs(with_one_time_cost(res, 10000000)["gain"] - r["gain"]) < 1e-12
     res["search"]["accepted_per_s_plain"] = 0.0
     assert with_one_time_cost(res)["gain"] is None

@@ -213,13 +213,13 @@ def test_search_pipeline_small():
     SRES on a small her_model_2014 case (50 cells, 200 minutes)."""
     from dense_b200 import search as S
     sim = dict(minutes=200.0, cells=50, width=5)
-    P = S.draw_candidates(768, 5)
+    P = S.draw_candidates(4096, 5)
     F = S.simulate_features(P, **sim)
     assert np.isfinite(F["period"]).sum() > 50
     assert F["oscillates"].sum() > 50
     syn = F["synchrony"][np.isfinite(F["synchrony"])]
     assert ((syn >= -1.0001) & (syn <= 1.0001)).all()
-    net = S.train_surrogate(P, F, epochs=60, batch=128)
+    net = S.train_surrogate(P, F, epochs=60, batch=512, ensemble=2)
     err = S.feature_errors(net, P, F)
     assert err["period_median"] < 0.5 and err["oscillation_accuracy"] > 0.6
     res = S.screened_search(net, 20000, 6, keep=0.01, plain_sample=2000, sim_kwargs=sim)
