@@ -80,26 +80,29 @@ def synchrony(traj):
     return float(((s * s).sum() - n) / (n * (n - 1)))
 
 
+def _kernels(device):
+    """The surrogate library's launchers on `device` (one per device)."""
+    from .surrogate import Kernels
+    k = _KERNELS.get(device)
+    if k is None:
+        k = _KERNELS[device] = Kernels(device)
+    return k
+
+
+_KERNELS = {}
+
+
 def synchrony_batch(X, counts):
-    """synchrony() of every set at once on the GPU: X [sets][samples][cells]
-    (a CUDA tensor; rows past a set's count are ignored), counts [sets];
-    float64, numpy array out."""
+    """synchrony() of every set at once on the GPU (one CTA per set,
+    csrc/surrogate/features.cu): X [sets][samples][cells] (a float64 CUDA
+    tensor, cells contiguous; rows past a set's count are ignored), counts
+    [sets]; float64 numpy array out."""
     import torch
-    B, T, Cn = X.shape
-    cnt = torch.as_tensor(np.asarray(counts), device=X.device, dtype=torch.float64)
-    w = (torch.arange(T, device=X.device)[None, :] < cnt[:, None]).to(X.dtype)[:, :, None]
-    mean = (X * w).sum(1, keepdim=True) / cnt.clamp(min=1)[:, None, None]
-    x = (X - mean) * w
-    nrm = torch.sqrt((x * x).sum(1))                                    # [B, C]
-    top = (X.abs() * w).amax(dim=(1, 2))                                 # [B]
-    ok = nrm > 1e-12 * (1.0 + top[:, None])
-    n = ok.sum(1).to(X.dtype)
-    z = torch.where(ok[:, None, :], x / torch.where(ok, nrm, torch.ones_like(nrm))[:, None, :],
-                    torch.zeros_like(x))
-    s = z.sum(2)                                                         # [B, T]
-    syn = ((s * s).sum(1) - n) / (n * (n - 1)).clamp(min=1)
-    syn = torch.where(n >= 2, syn, torch.full_like(syn, float("nan")))
-    return syn.cpu().numpy()
+    k = _kernels(X.device.index or 0)
+    cnt = torch.as_tensor(np.asarray(counts, np.int32), device=X.device)
+    out = torch.empty(X.shape[0], dtype=torch.float64, device=X.device)
+    k.synchrony(X, cnt, out)
+    return out.cpu().numpy()
 
 
 def simulate_features(P, minutes=None, cells=200, width=4, window=60.0, batch=4096, device=0,
@@ -233,15 +236,15 @@ REGION_WEIGHT = 0.1   # weight of the predicted features' closeness to the accep
 AMP_RAMP = 0.1        # log-amplitude width over which the amplitude term rises from 0 to 1
 
 
-def _region_terms(log_per, log_amp, p_osc, xp):
+def _region_terms(log_per, log_amp, p_osc):
     """Closeness of the predicted features to the acceptance region: minus
     the period's distance from the target in tolerances, plus half a ramp
     in log amplitude around AMP_MIN and half the oscillation indicator
-    (both clipped to [0, 1]); `xp` is numpy or torch."""
-    clip = (lambda x, lo, hi: xp.clip(x, lo, hi)) if xp is np else (lambda x, lo, hi: x.clamp(lo, hi))
-    per = xp.exp(clip(log_per, -10.0, 10.0))
-    amp_term = clip((log_amp - math.log(AMP_MIN)) / AMP_RAMP + 0.5, 0.0, 1.0)
-    return -xp.abs(per - TARGET_PERIOD) / PERIOD_TOL + 0.5 * amp_term + 0.5 * clip(p_osc, 0.0, 1.0)
+    (both clipped to [0, 1]).  The GPU form is score_kernel in
+    csrc/surrogate/features.cu."""
+    per = np.exp(np.clip(log_per, -10.0, 10.0))
+    amp_term = np.clip((log_amp - math.log(AMP_MIN)) / AMP_RAMP + 0.5, 0.0, 1.0)
+    return -np.abs(per - TARGET_PERIOD) / PERIOD_TOL + 0.5 * amp_term + 0.5 * np.clip(p_osc, 0.0, 1.0)
 
 
 def predicted_score(pred):
@@ -250,26 +253,44 @@ def predicted_score(pred):
     region (the two together keep more of the candidates the FP64
     simulation accepts than either alone)."""
     pred = np.asarray(pred, np.float64)
-    return pred[:, 4] + REGION_WEIGHT * _region_terms(pred[:, 0], pred[:, 1], pred[:, 3], np)
+    return pred[:, 4] + REGION_WEIGHT * _region_terms(pred[:, 0], pred[:, 1], pred[:, 3])
 
 
-def score_candidates(net, P, chunk=1 << 20, spread=SPREAD):
-    """predicted_score(net.predict(encode(P))) with the encoding, the
-    network and the score on the GPU, chunk by chunk; float64 numpy array."""
+def score_candidates(net, P, chunk=1 << 20, spread=SPREAD, batch=65536):
+    """predicted_score(net.predict(encode(P))) on the GPU: per chunk of
+    candidates one host-to-device copy of their parameters, then the
+    encoding, every network of the ensemble (`net` a Surrogate, or one MLP)
+    and the score in the surrogate library's kernels; float64 numpy array."""
     import torch
-    dev = net.dev
-    t = template()
+    from .surrogate import IN_PAD
+    nets = getattr(net, "nets", None) or [net]
+    n_out = nets[0].n_out
+    mu = getattr(net, "mu", np.zeros(n_out, np.float32))
+    sd = getattr(net, "sd", np.ones(n_out, np.float32))
+    dev = nets[0].dev
+    k = nets[0].k
     idx = active_params()
-    tt = torch.as_tensor(t[idx], device=dev, dtype=torch.float64)
-    it = torch.as_tensor(idx, device=dev)
-    out = []
-    for s in range(0, P.shape[0], chunk):
-        # whole rows across (a contiguous slice, no host copy), columns picked on the GPU
-        x = torch.as_tensor(P[s:s + chunk], device=dev)[:, it]
-        x = (torch.log(x / tt) / math.log(spread)).to(torch.float32)
-        y = net.predict_device(x).to(torch.float64)
-        out.append((y[:, 4] + REGION_WEIGHT * _region_terms(y[:, 0], y[:, 1], y[:, 3], torch)).cpu().numpy())
-    return np.concatenate(out) if out else np.zeros(0)
+    idx_d = torch.as_tensor(idx.astype(np.int32), device=dev)
+    t_d = torch.as_tensor(template()[idx], device=dev, dtype=torch.float64)
+    for m in nets:
+        m._cast_weights()
+    n = P.shape[0]
+    out = torch.empty(n, dtype=torch.float64, device=dev)
+    acc = torch.empty((batch, n_out), dtype=torch.float32, device=dev)
+    for s in range(0, n, chunk):
+        Pd = torch.as_tensor(np.ascontiguousarray(P[s:s + chunk], np.float64), device=dev)
+        for b in range(0, Pd.shape[0], batch):
+            rows = min(batch, Pd.shape[0] - b)
+            Bp = (rows + 127) // 128 * 128
+            Xb = nets[0]._buf("Xscore", (Bp, IN_PAD), torch.bfloat16)
+            k.encode(Pd[b:b + rows], idx_d, t_d, math.log(spread), Xb)
+            for i, m in enumerate(nets):
+                k.ensemble_accumulate(m.forward(Xb), rows, n_out, acc, i == 0)
+            k.score(acc[:rows], len(nets), mu, sd, REGION_WEIGHT, TARGET_PERIOD, PERIOD_TOL, AMP_MIN, AMP_RAMP,
+                    out[s + b:s + b + rows])
+    for m in nets:
+        m.k.check()
+    return out.cpu().numpy()
 
 
 def feature_errors(net, P, F):

@@ -37,12 +37,17 @@ def build(force=False):
     if not force and os.path.exists(LIB) and all(os.path.getmtime(s) <= os.path.getmtime(LIB) for s in srcs):
         return LIB
     os.makedirs(os.path.join(LIB_DIR, "obj"), exist_ok=True)
-    obj = os.path.join(LIB_DIR, "obj", "mlp.o")
     nvcc = os.environ.get("NVCC", "nvcc")
     base = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O3", "-lineinfo"]
-    for cmd in (base + ["-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-c",
-                        os.path.join(SRC, "mlp.cu"), "-o", obj],
-                base + ["-shared", "-o", LIB, obj, "-lcudart"]):
+    objs = []
+    cmds = []
+    for unit in ("mlp", "features"):
+        obj = os.path.join(LIB_DIR, "obj", unit + ".o")
+        objs.append(obj)
+        cmds.append(base + ["-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-c",
+                            os.path.join(SRC, unit + ".cu"), "-o", obj])
+    cmds.append(base + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    for cmd in cmds:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             raise RuntimeError(r.stderr[-4000:])
@@ -68,6 +73,11 @@ def lib():
         L.dense_mlp_adam_dev.argtypes = [vp, vp, vp, vp, i64, vp, vp]
         L.dense_mlp_mse_dev.argtypes = [vp, i, vp, vp, i, i, vp, vp, vp, vp, vp]
         L.dense_mlp_gather.argtypes = [vp, i, i, vp, vp, i, vp, i, i, vp, i, vp, vp, vp]
+        L.dense_features_synchrony.argtypes = [vp, i64, i64, i, vp, i, vp, vp]
+        L.dense_features_encode.argtypes = [vp, i, i, vp, vp, i, C.c_double, vp, i, i, vp]
+        L.dense_features_ensemble_accumulate.argtypes = [vp, i, i, i, vp, i, vp]
+        L.dense_features_score.argtypes = [vp, i, i, i, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, vp, vp]
         _lib = L
     return _lib
 
@@ -141,6 +151,39 @@ class Kernels:
     def adam_dev(self, w, g, m, v, hyper):
         """adam with {lr, b1, b2, eps, 1 - b1^t, 1 - b2^t} in device memory."""
         assert self.L.dense_mlp_adam_dev(_p(w), _p(g), _p(m), _p(v), w.numel(), _p(hyper), self._s()) == 0
+
+    def synchrony(self, X, counts, out):
+        """Mean pairwise Pearson correlation across cells per set: X a
+        float64 CUDA tensor [sets][samples][cells] (cells contiguous; any
+        set and sample strides), counts int32 [sets] (samples per set),
+        out float64 [sets]."""
+        B, _, cells = X.shape
+        assert X.stride(2) == 1
+        assert self.L.dense_features_synchrony(_p(X), X.stride(0), X.stride(1), cells, _p(counts), B, _p(out),
+                                               self._s()) == 0
+
+    def encode(self, P, idx, tmpl, log_spread, Xb):
+        """Network inputs of candidates P (float64 [n][params]) into BF16
+        Xb [Bp][in_pad]: log(P[:, idx] / tmpl) / log_spread, zero padded."""
+        n, ldp = P.shape
+        Bp, in_pad = Xb.shape
+        assert P.stride(1) == 1
+        assert self.L.dense_features_encode(_p(P), P.stride(0), n, _p(idx), _p(tmpl), idx.shape[0], float(log_spread),
+                                            _p(Xb), in_pad, Bp, self._s()) == 0
+
+    def ensemble_accumulate(self, Y, n, nout, acc, first):
+        assert self.L.dense_features_ensemble_accumulate(_p(Y), Y.stride(0), n, nout, _p(acc), int(first),
+                                                         self._s()) == 0
+
+    def score(self, acc, nets, mu, sd, weight, period, tol, amp_min, ramp, out):
+        """Ranking score from the ensemble sum acc [n][nout] (see
+        csrc/surrogate/features.cu); mu and sd numpy float32 [nout]."""
+        n, nout = acc.shape
+        mu = np.ascontiguousarray(mu, np.float32)
+        sd = np.ascontiguousarray(sd, np.float32)
+        assert self.L.dense_features_score(_p(acc), n, nout, nets, mu.ctypes.data_as(C.c_void_p),
+                                           sd.ctypes.data_as(C.c_void_p), weight, period, tol, amp_min, ramp, _p(out),
+                                           self._s()) == 0
 
     def colsum(self, dZ, db):
         r, c = dZ.shape

@@ -244,6 +244,44 @@ def test_synchrony_known_answers():
     assert abs(synchrony(anti) + 1.0) < 1e-12
 
 
+def test_synchrony_kernel_matches_numpy():
+    """The per-set synchrony kernel against search.synchrony on trajectories
+    with different sample counts, a constant cell, an all-constant set, a
+    set with a NaN sample and a set with no samples, read through a strided
+    view [sets][samples][species 1 of 2][cells]."""
+    import torch
+    from dense_b200 import search as S
+    rng = np.random.Generator(np.random.PCG64(12))
+    sets, cap, cells = 7, 90, 37
+    X = rng.normal(size=(sets, cap, 2, cells))
+    t = np.arange(cap)[:, None]
+    X[:, :, 1, :] = np.sin(0.2 * t + rng.uniform(0, 0.5, size=(1, cells))) + 0.1 * X[:, :, 1, :]
+    X[1, :, 1, 5] = 3.0            # a constant cell
+    X[2, :, 1, :] = 1.5            # every cell constant
+    X[3, 17, 1, 4] = np.nan        # a NaN sample
+    counts = np.array([90, 60, 90, 90, 1, 0, 33], np.int32)
+    got = S.synchrony_batch(torch.tensor(X, device="cuda")[:, :, 1, :], counts)
+    for i in range(sets):
+        want = S.synchrony(X[i, :counts[i], 1, :]) if counts[i] > 0 else float("nan")
+        if np.isnan(want):
+            assert np.isnan(got[i]), (i, got[i])
+        else:
+            assert abs(got[i] - want) < 1e-12, (i, got[i], want)
+
+
+def test_ensemble_scoring_on_the_gpu_matches_the_host():
+    """score_candidates with a two-network Surrogate (standardised outputs)
+    against predicted_score(Surrogate.predict(encode(P)))."""
+    from dense_b200 import search as S
+    from dense_b200.surrogate import MLP
+    nets = [MLP(len(S.active_params()), 5, seed=s) for s in (3, 4)]
+    sur = S.Surrogate(nets, mu=[3.3, 3.9, 0.2, 0.0, 0.0], sd=[0.4, 0.8, 0.3, 1.0, 1.0])
+    P = S.draw_candidates(3000, 8)
+    host = S.predicted_score(sur.predict(S.encode(P)))
+    dev = S.score_candidates(sur, P, chunk=1024, batch=512)
+    assert np.max(np.abs(host - dev)) < 1e-4
+
+
 def test_sharded_screening_single_rank_matches_direct_resimulation():
     """The multi-GPU screening path on one process: the top k of the scored
     candidate range, re-simulated, gives the accepted count a direct
