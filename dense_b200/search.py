@@ -159,6 +159,18 @@ def accepted(F):
         return np.isfinite(per) & (np.abs(per - TARGET_PERIOD) <= PERIOD_TOL) & (np.nan_to_num(amp) >= AMP_MIN)
 
 
+def merge_features(*Fs):
+    """One feature dict from several simulate_features results: the per-set
+    arrays concatenated in order, seconds and cell-steps summed."""
+    out = {}
+    for key in Fs[0]:
+        if key in ("seconds", "cell_steps"):
+            out[key] = sum(F[key] for F in Fs)
+        else:
+            out[key] = np.concatenate([np.asarray(F[key]) for F in Fs])
+    return out
+
+
 def targets(F):
     """Surrogate targets [n][5]: log period, log amplitude, synchrony, the
     oscillation indicator and the acceptance indicator; and their mask

@@ -117,3 +117,12 @@ def test_gain_with_one_time_cost():
     assert abs(with_one_time_cost(res, 10000000)["gain"] - r["gain"]) < 1e-12
     res["search"]["accepted_per_s_plain"] = 0.0
     assert with_one_time_cost(res)["gain"] is None
+
+
+def test_merge_features_concatenates_in_order():
+    from dense_b200.search import merge_features
+    a = {"period": np.array([1.0, 2.0]), "status": np.array([0, 1], np.int32), "seconds": 1.5, "cell_steps": 10}
+    b = {"period": np.array([3.0]), "status": np.array([2], np.int32), "seconds": 0.5, "cell_steps": 4}
+    m = merge_features(a, b)
+    assert m["period"].tolist() == [1.0, 2.0, 3.0] and m["status"].tolist() == [0, 1, 2]
+    assert m["seconds"] == 2.0 and m["cell_steps"] == 14
