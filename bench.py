@@ -645,6 +645,7 @@ def main():
     # ---- e2e through the public API, host buffers
     e2e_times = []
     h2d = d2h = 0
+    e2e_clocks = Clocks(local)
     for k in range(a.e2e_steps):
         barrier()
         t0 = time.perf_counter()
@@ -662,6 +663,7 @@ def main():
             h2d = sum(s.set_params.nbytes + (s.cell_params.nbytes if s.cell_params is not None else 0) +
                       s.nbr_offsets.nbytes + s.nbr_ids.nbytes for s in sets)
             d2h = sum(r.nbytes for r in res)
+    e2e_clk = e2e_clocks.stop()
     # per rank the median of the e2e steps, then the slowest rank
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     if world > 1:
@@ -702,7 +704,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": a.e2e_steps,
-                    "step_s": [round(x, 4) for x in e2e_times],
+                    "step_s": [round(x, 4) for x in e2e_times], "clocks": e2e_clk,
                     "what": "Batch() from host arrays + full horizon + every set's oscillation amplitudes and "
                             "periods to host; median of the steps"},
             "gpu_launches": a.steps,
