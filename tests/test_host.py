@@ -38,6 +38,29 @@ def test_surrogate_library_exports_its_entry_points():
         assert hasattr(lib, name), name
 
 
+def test_surrogate_entry_points_refuse_bad_arguments_on_the_host():
+    """Shape and argument checks return 1 before any CUDA call (so they run
+    without a GPU): rows not a multiple of 128, N outside [16, 256], K not a
+    multiple of 64, a bias epilogue without a bias, too many cells for the
+    synchrony kernel, bad encode and score arguments."""
+    from dense_b200 import surrogate
+    L = ctypes.CDLL(surrogate.build())
+    vp, i, i64, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+    L.dense_mlp_gemm_ws.argtypes = [vp, i, vp, i, vp, i, i, i, i, i, vp, vp, i, vp, vp, ctypes.c_size_t, vp]
+    p = vp(16)  # never dereferenced: every call below is refused first
+    for M, N, K, epi, bias in ((100, 64, 64, 0, None), (128, 8, 64, 0, None), (128, 512, 64, 0, None),
+                               (128, 64, 96, 0, None), (128, 64, 64, 2, None), (128, 64, 64, 3, p)):
+        assert L.dense_mlp_gemm_ws(p, K, p, K, p, N, M, N, K, epi, bias, p, N, p, None, 0, None) == 1
+    L.dense_features_synchrony.argtypes = [vp, i64, i64, i, vp, i, vp, vp]
+    assert L.dense_features_synchrony(p, 0, 0, 2048, p, 1, p, None) == 1
+    L.dense_features_encode.argtypes = [vp, i, i, vp, vp, i, d, vp, i, i, vp]
+    assert L.dense_features_encode(p, 45, 10, p, p, 80, 1.386, p, 64, 128, None) == 1   # k > in_pad
+    assert L.dense_features_encode(p, 45, 200, p, p, 44, 1.386, p, 64, 128, None) == 1  # n > Bp
+    L.dense_features_score.argtypes = [vp, i, i, i, vp, vp, d, d, d, d, d, vp, vp]
+    assert L.dense_features_score(p, 10, 4, 1, p, p, 0.1, 30.0, 3.0, 50.0, 0.1, p, None) == 1  # nout < 5
+    assert L.dense_features_score(p, 10, 5, 0, p, p, 0.1, 30.0, 3.0, 50.0, 0.1, p, None) == 1  # no networks
+
+
 def test_model_info_matches_oracle():
     from dense_b200.engine import load
     from oracle.pyoracle import load_oracle
