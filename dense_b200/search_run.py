@@ -15,7 +15,7 @@ Prints one JSON object.  Usage:
   python -m dense_b200.search_run [--train N] [--test N] [--candidates N]
       [--minutes M] [--resim-minutes R[,R2...]] [--cells C] [--epochs E]
       [--ensemble K] [--generations G] [--extrapolate N[,N2...]]
-      [--refine K [--refine-pool N]] [--data-cache FILE]
+      [--refine K [--refine-pool N] [--refine-rounds R]] [--data-cache FILE]
 
 --minutes is the horizon of the training and held-out simulations (the
 features' window is 0-60 min, and the first 60 minutes of a run do not
@@ -104,6 +104,7 @@ def main(argv=None):
                     help="candidates the first network ranks best in a fresh pool, simulated and added to the "
                          "training set before the networks are trained again (0: no refinement)")
     ap.add_argument("--refine-pool", type=int, default=2000000)
+    ap.add_argument("--refine-rounds", type=int, default=1)
     ap.add_argument("--extrapolate", default="58000000",
                     help="candidate counts for the charged gain scaled from the measured run, comma-separated")
     ap.add_argument("--data-cache", default=None,
@@ -126,22 +127,22 @@ def main(argv=None):
     net = S.train_surrogate(P_train, F_train, epochs=a.epochs, batch=2048, seed=a.seed, log=log,
                             ensemble=a.ensemble)
     res["training_s"] = time.perf_counter() - t1
-    if a.refine > 0:
-        # one round of refinement: the first network ranks a fresh pool, its
+    res["refine"] = []
+    for r in range(a.refine_rounds if a.refine > 0 else 0):
+        # a round of refinement: the current networks rank a fresh pool, its
         # best `refine` candidates are simulated and join the training set
         # (they lie where the search looks), and the networks are trained
         # again on everything; all of it counts in the one-time cost
         t2 = time.perf_counter()
-        pool = S.draw_candidates(a.refine_pool, a.seed + 3)
+        pool = S.draw_candidates(a.refine_pool, a.seed + 3 + r)
         top = np.argpartition(-S.score_candidates(net, pool), a.refine)[:a.refine]
         F_ref = S.simulate_features(pool[top], log=log, **sim)
-        first_accept = float(S.accepted(F_ref).mean())
         P_train = np.concatenate([P_train, pool[top]])
         F_train = S.merge_features(F_train, F_ref)
         net = S.train_surrogate(P_train, F_train, epochs=a.epochs, batch=2048, seed=a.seed, log=log,
                                 ensemble=a.ensemble)
-        res["refine"] = {"pool": a.refine_pool, "simulated": a.refine, "seconds": F_ref["seconds"],
-                         "accepted_fraction_of_simulated": first_accept}
+        res["refine"].append({"pool": a.refine_pool, "simulated": a.refine, "seconds": F_ref["seconds"],
+                              "accepted_fraction_of_simulated": float(S.accepted(F_ref).mean())})
         res["training_s"] += time.perf_counter() - t2 - F_ref["seconds"]
         res["data"]["train_sets"] = len(P_train)
         res["data"]["seconds"] += F_ref["seconds"]
