@@ -104,7 +104,7 @@ def main(argv=None):
                     help="candidates the first network ranks best in a fresh pool, simulated and added to the "
                          "training set before the networks are trained again (0: no refinement)")
     ap.add_argument("--refine-pool", type=int, default=2000000)
-    ap.add_argument("--refine-rounds", type=int, default=1)
+    ap.add_argument("--refine-rounds", type=int, default=3)
     ap.add_argument("--extrapolate", default="58000000",
                     help="candidate counts for the charged gain scaled from the measured run, comma-separated")
     ap.add_argument("--data-cache", default=None,
