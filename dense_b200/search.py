@@ -214,7 +214,7 @@ def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, grou
     `standardize_indicators`, which weighs the rare acceptances up); with a
     process group, data-parallel over the ranks' shards (gradients averaged
     every step)."""
-    from .surrogate import MLP
+    from .surrogate import MLP, fit_concurrently
     X = encode(P)
     T, M = targets(F)
     mu = np.zeros(T.shape[1], np.float32)
@@ -235,12 +235,16 @@ def train_surrogate(P, F, epochs=30, batch=4096, seed=0, lr=1e-3, log=None, grou
         t = (t / dist.get_world_size(group)).cpu().numpy().astype(np.float32)
         mu, sd = t[:T.shape[1]], t[T.shape[1]:]
     Ts = ((T - mu) / sd) * M
-    nets = []
-    for k in range(ensemble):
-        net = MLP(X.shape[1], T.shape[1], seed=seed + 1000 * k, lr=lr, group=group, device=device)
-        net.fit(X, Ts, M, epochs=epochs, batch=min(batch, (X.shape[0] // 128) * 128), seed=seed + 1000 * k,
-                log=log)
-        nets.append(net)
+    nets = [MLP(X.shape[1], T.shape[1], seed=seed + 1000 * k, lr=lr, group=group, device=device)
+            for k in range(ensemble)]
+    b = min(batch, (X.shape[0] // 128) * 128)
+    if group is None and ensemble > 1:
+        # the ensemble's networks train at once, one CUDA stream each
+        fit_concurrently(nets, X, Ts, M, [seed + 1000 * k for k in range(ensemble)], epochs=epochs, batch=b,
+                         log=log)
+    else:
+        for k, net in enumerate(nets):
+            net.fit(X, Ts, M, epochs=epochs, batch=b, seed=seed + 1000 * k, log=log)
     return Surrogate(nets, mu, sd)
 
 

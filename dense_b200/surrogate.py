@@ -415,16 +415,20 @@ class MLP:
                 g["update"].append(gu)
         return g
 
-    def _fit_captured(self, X, T, mask, n, epochs, batch, rng, log, cosine, b1=0.9, b2=0.999, eps=1e-8):
+    def _fit_epochs(self, X, T, mask, n, epochs, batch, rng, cosine, data=None, b1=0.9, b2=0.999, eps=1e-8):
+        """Generator behind the captured fit: each next() enqueues one epoch
+        on the current stream and returns a function that reads that
+        epoch's mean loss (call it before the next epoch is enqueued).
+        `data`: the training set already on the device (X, T, mask)."""
         torch = self.torch
         steps = n // batch
-        hist = []
         if steps == 0:
-            return [0.0] * epochs
-        Xd = torch.as_tensor(np.ascontiguousarray(X, dtype=np.float32), device=self.dev)
-        Td = torch.as_tensor(np.ascontiguousarray(np.nan_to_num(T), dtype=np.float32), device=self.dev)
-        Md = torch.as_tensor(np.ascontiguousarray(mask, dtype=np.float32), device=self.dev)
-        g = self._train_graphs((Xd, Td, Md), batch, steps)
+            for _ in range(epochs):
+                yield lambda: 0.0
+            return
+        if data is None:
+            data = device_training_set(X, T, mask, self.dev)
+        g = self._train_graphs(data, batch, steps)
         lr0 = self.lr
         total = epochs * steps
         for ep in range(epochs):
@@ -450,11 +454,16 @@ class MLP:
                     average_(g["dW"] + g["db"], self.group)
                     g["update"][j].replay()
             self.steps += steps
-            hist.append(float(g["loss"].item()) / steps)
+            yield lambda: float(g["loss"].item()) / steps
+        del g
+
+    def _fit_captured(self, X, T, mask, n, epochs, batch, rng, log, cosine):
+        hist = []
+        for ep, loss in enumerate(self._fit_epochs(X, T, mask, n, epochs, batch, rng, cosine)):
+            hist.append(loss())
             self.k.check()
             if log:
                 log("epoch %d loss %.5f" % (ep, hist[-1]))
-        del g
         return hist
 
     def step(self, X, T, mask):
@@ -505,6 +514,51 @@ class MLP:
 
     def state(self):
         return {"W": [w.cpu().numpy() for w in self.W], "b": [b.cpu().numpy() for b in self.b]}
+
+
+def device_training_set(X, T, mask, dev):
+    """The training set on the device as float32 tensors (NaN targets 0)."""
+    import torch
+    return (torch.as_tensor(np.ascontiguousarray(X, dtype=np.float32), device=dev),
+            torch.as_tensor(np.ascontiguousarray(np.nan_to_num(T), dtype=np.float32), device=dev),
+            torch.as_tensor(np.ascontiguousarray(mask, dtype=np.float32), device=dev))
+
+
+def fit_concurrently(nets, X, T, mask, seeds, epochs=20, batch=4096, log=None, cosine=True):
+    """MLP.fit of several networks of one process at once, each on its own
+    CUDA stream (a network's epoch is one graph replay; the GEMMs of one
+    4096-row batch fill only a few dozen SMs, so the networks share the
+    GPU).  Network k takes the batches of seed seeds[k]: its weights are
+    those of nets[k].fit(..., seed=seeds[k]).  Returns the loss histories."""
+    import torch
+    assert all(net.group is None for net in nets)
+    dev = nets[0].dev
+    data = device_training_set(X, T, mask, dev)
+    n = X.shape[0]
+    streams = [torch.cuda.Stream(dev) for _ in nets]
+    for st in streams:
+        st.wait_stream(torch.cuda.current_stream(dev))
+    gens = [net._fit_epochs(X, T, mask, n, epochs, batch, np.random.Generator(np.random.PCG64(sd)), cosine,
+                            data=data) for net, sd in zip(nets, seeds)]
+    hists = [[] for _ in nets]
+    for ep in range(epochs):
+        readers = []
+        for gen, st in zip(gens, streams):
+            with torch.cuda.stream(st):
+                readers.append(next(gen))
+        for k, (read, st) in enumerate(zip(readers, streams)):
+            with torch.cuda.stream(st):
+                hists[k].append(read())
+        for net in nets:
+            net.k.check()
+        if log:
+            log("epoch %d loss %s" % (ep, " ".join("%.5f" % h[-1] for h in hists)))
+    for gen in gens:
+        gen.close()
+    torch.cuda.current_stream(dev).wait_stream(streams[0])
+    for st in streams[1:]:
+        torch.cuda.current_stream(dev).wait_stream(st)
+    return hists
 
 
 def bench_gemm(rows=131072, reps=20, device=0):

@@ -143,6 +143,26 @@ def test_captured_training_follows_the_launched_steps():
         assert d < 1e-3, d
 
 
+def test_concurrent_ensemble_training_equals_one_by_one():
+    """Networks trained at once on separate streams end with the weights of
+    the same networks trained one after the other (every kernel of a step
+    is deterministic)."""
+    from dense_b200.surrogate import MLP, fit_concurrently
+    rng = np.random.Generator(np.random.PCG64(10))
+    X = rng.uniform(-1, 1, size=(5000, 12)).astype(np.float32)
+    T = np.stack([np.sin(X[:, 0]), X[:, 1] * X[:, 2]], 1).astype(np.float32)
+    M = np.ones_like(T)
+    seq = [MLP(12, 2, seed=s) for s in (1, 2, 3)]
+    for net, s in zip(seq, (11, 12, 13)):
+        net.fit(X, T, M, epochs=3, batch=1024, seed=s)
+    con = [MLP(12, 2, seed=s) for s in (1, 2, 3)]
+    hists = fit_concurrently(con, X, T, M, [11, 12, 13], epochs=3, batch=1024)
+    assert len(hists) == 3 and all(len(h) == 3 for h in hists)
+    for a, b in zip(seq, con):
+        for wa, wb in zip(a.W + a.b, b.W + b.b):
+            assert (wa == wb).all()
+
+
 def test_umma_gemm_bias_gelu_epilogue():
     import torch
     from dense_b200.surrogate import EPI_BIAS, EPI_BIAS_GELU, Kernels
