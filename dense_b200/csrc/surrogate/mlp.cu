@@ -363,6 +363,8 @@ int try_persistent(const void* A, int lda, const void* B, int ldb, float* D, int
   const int n_chunks = K / kChunkK;
   a.splits = 1;
   a.chunks_per_split = n_chunks;
+  a.nsplit = 1;
+  a.n_blk = N;
   // split K when the row tiles leave most SMs idle and K is long: at least
   // four chunks per unit, partials in the caller's workspace
   if (ws && aligned16(ws) && a.tiles * 2 <= sms && n_chunks >= 8) {
@@ -376,6 +378,13 @@ int try_persistent(const void* A, int lda, const void* B, int ldb, float* D, int
       a.chunks_per_split = cps;
     }
   }
+  // without a K split, few row tiles take column blocks instead (at least
+  // 64 columns each), so that more SMs share the product
+  if (a.splits == 1) {
+    while (a.tiles * a.nsplit * 2 <= sms && (N / (a.nsplit * 2)) % kStoreBox == 0 && N / (a.nsplit * 2) >= 64)
+      a.nsplit *= 2;
+    a.n_blk = N / a.nsplit;
+  }
   const int kernel_epi = a.splits > 1 ? kEpiStore : epilogue;
   const size_t limit = kernel_epi == kEpiStore      ? persistent_smem_limit<kEpiStore>()
                        : kernel_epi == kEpiBiasGelu ? persistent_smem_limit<kEpiBiasGelu>()
@@ -383,7 +392,7 @@ int try_persistent(const void* A, int lda, const void* B, int ldb, float* D, int
   const size_t smem = persistent_smem(a, kernel_epi, limit);
   if (!smem) return 1;
   CUtensorMap ma, mb, md, mh;
-  if (!bf16_map(&ma, A, M, K, lda, kTileM) || !bf16_map(&mb, B, N, K, ldb, N)) return 1;
+  if (!bf16_map(&ma, A, M, K, lda, kTileM) || !bf16_map(&mb, B, N, K, ldb, a.n_blk)) return 1;
   const bool mapped = a.splits > 1 ? store_map(&md, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ws, a.splits * M, N, N,
                                                kStoreBox, kStoreBox, CU_TENSOR_MAP_SWIZZLE_128B)
                                    : store_map(&md, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, D, M, N, ldd, kStoreBox,
@@ -396,7 +405,7 @@ int try_persistent(const void* A, int lda, const void* B, int ldb, float* D, int
   } else {
     mh = md;
   }
-  const int units = a.tiles * a.splits;
+  const int units = a.tiles * a.splits * a.nsplit;
   const int grid = units < sms ? units : sms;
   cudaError_t e = kernel_epi == kEpiStore ? launch_persistent<kEpiStore>(ma, mb, md, mh, a, smem, grid, s)
                   : kernel_epi == kEpiBiasGelu

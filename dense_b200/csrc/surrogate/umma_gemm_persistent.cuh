@@ -4,7 +4,9 @@
 //   D[M][N] (FP32) = A[M][K] . B[N][K]^T (+ bias, GELU -> H in BF16)
 //
 // One CTA per SM walks the work units u = blockIdx.x, += gridDim.x.  A unit
-// is a 128-row tile of D, or with split-K a tile and a range of K chunks.
+// is a 128-row tile of D, or with split-K a tile and a range of K chunks,
+// or with column blocks (few row tiles, K too short to split) a tile and a
+// block of N / nsplit columns.
 // Ten warps with fixed roles:
 //
 //   warp 0     one thread drives the Tensor Memory Accelerator: A chunks of
@@ -52,7 +54,9 @@ constexpr uint32_t kStageH = kStoreBox * kStoreBox * 2;  // BF16 staging box, 64
 struct PersistentArgs {
   int M, N, K;
   int tiles;             // M / 128
-  int splits;            // units per tile (1: no split)
+  int splits;            // K ranges per tile (1: no split)
+  int nsplit;            // column blocks per tile (1: the whole N)
+  int n_blk;             // columns of one block, N / nsplit (a multiple of 32)
   int chunks_per_split;  // K chunks of 64 per unit
   int stages;            // shared-memory ring depth
   int resident_b;        // B loaded once for the whole launch
@@ -74,8 +78,8 @@ struct PersistentArgs {
 inline size_t persistent_smem(PersistentArgs& a, int epi, size_t limit) {
   if (limit < 1024 + kADim) return 0;
   const size_t room = limit - 1024;
-  const size_t b_all = static_cast<size_t>(a.N) * static_cast<size_t>(a.K) * 2;
-  const size_t b_chunk = static_cast<size_t>(a.N) * kChunkK * 2;
+  const size_t b_all = static_cast<size_t>(a.n_blk) * static_cast<size_t>(a.K) * 2;
+  const size_t b_chunk = static_cast<size_t>(a.n_blk) * kChunkK * 2;
   const size_t per_buf = kStageD + (epi == kEpiBiasGelu ? kStageH : 0);
   struct Option {
     bool resident;
@@ -87,7 +91,7 @@ inline size_t persistent_smem(PersistentArgs& a, int epi, size_t limit) {
     const size_t b_bytes = o.resident ? ((b_all + 1023) & ~static_cast<size_t>(1023)) : 0;
     const size_t stage = kADim + (o.resident ? 0 : b_chunk);
     const int min_stages = o.resident ? 3 : 2;
-    if (o.resident && (a.splits > 1 || b_all > 128 * 1024)) continue;
+    if (o.resident && (a.splits > 1 || a.nsplit > 1 || b_all > 128 * 1024)) continue;
     if (staging + b_bytes + min_stages * stage > room) continue;
     int st = static_cast<int>((room - staging - b_bytes) / stage);
     if (st > kMaxStages) st = kMaxStages;
@@ -161,9 +165,11 @@ __global__ void __launch_bounds__(kPersThreads, 1)
   __shared__ float s_bias[256];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int N = p.N, S = p.stages, splits = p.splits, cps = p.chunks_per_split;
+  // N: the columns of one unit's accumulator (a block of the output's)
+  const int N = p.n_blk, S = p.stages, splits = p.splits, cps = p.chunks_per_split, nsplit = p.nsplit;
   const int n_chunks = p.K / kChunkK;
-  const int units = p.tiles * splits;
+  const int per_tile = splits * nsplit;  // units per 128-row tile: K ranges x column blocks
+  const int units = p.tiles * per_tile;
   // the 128-byte swizzle of the staging boxes repeats every 1024 bytes of
   // shared-memory address: the layout starts on such a boundary
   unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(kPersThreads, 1)
     abort_flag = 0;
   }
   if (EPI != kEpiStore)
-    for (int i = tid; i < N; i += kPersThreads) s_bias[i] = p.bias[i];
+    for (int i = tid; i < p.N; i += kPersThreads) s_bias[i] = p.bias[i];
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(kPersThreads, 1)
           tma_load_2d(smem_u32(sBres + static_cast<size_t>(g) * N * 16), &tmB, g * 8, 0, bar);
       }
       for (int u = blockIdx.x; u < units && !bad; u += gridDim.x) {
-        const int tile = u / splits, c0 = (u % splits) * cps;
+        const int tile = u / per_tile, c0 = ((u % per_tile) / nsplit) * cps, nb = u % nsplit;
         const int c1 = min(c0 + cps, n_chunks);
         for (int c = c0; c < c1; ++c, ++it) {
           const int s = static_cast<int>(it % static_cast<uint32_t>(S));
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(kPersThreads, 1)
             unsigned char* sB = sA + kADim;
 #pragma unroll
             for (int j = 0; j < kChunkK / 8; ++j)
-              tma_load_2d(smem_u32(sB + j * N * 16), &tmB, c * kChunkK + j * 8, 0, fb);
+              tma_load_2d(smem_u32(sB + j * N * 16), &tmB, c * kChunkK + j * 8, nb * N, fb);
           }
         }
       }
@@ -266,7 +272,7 @@ __global__ void __launch_bounds__(kPersThreads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t acc = tmem + static_cast<uint32_t>(a * N);
-        const int c0 = (u % splits) * cps;
+        const int c0 = ((u % per_tile) / nsplit) * cps;
         const int c1 = min(c0 + cps, n_chunks);
         for (int c = c0; c < c1; ++c, ++it) {
           const int s = static_cast<int>(it % static_cast<uint32_t>(S));
@@ -325,7 +331,7 @@ __global__ void __launch_bounds__(kPersThreads, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int tile = u / splits, split = u % splits;
+      const int tile = u / per_tile, split = (u % per_tile) / nsplit, col0 = (u % nsplit) * N;
       const int out_row = split * p.M + tile * kTileM + q * 32;  // first row of this warp's boxes
       const uint32_t tacc = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(a * N);
       if (half >= n_groups) {  // no column group for this warp (N = 32)
@@ -345,7 +351,7 @@ __global__ void __launch_bounds__(kPersThreads, 1)
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[a])) : "memory");
         }
         float v[32];
-        epilogue_values<EPI>(r, s_bias, c0, v);
+        epilogue_values<EPI>(r, s_bias, col0 + c0, v);
         const int buf = static_cast<int>(groups % static_cast<uint32_t>(p.out_bufs));
         // the store issued from this buffer last time has read it
         if (lane == 0) {
@@ -377,8 +383,8 @@ __global__ void __launch_bounds__(kPersThreads, 1)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
         if (lane == 0) {
-          tma_store_2d(&tmD, c0, out_row, smem_u32(bd));
-          if (EPI == kEpiBiasGelu) tma_store_2d(&tmH, c0, out_row, smem_u32(bh));
+          tma_store_2d(&tmD, col0 + c0, out_row, smem_u32(bd));
+          if (EPI == kEpiBiasGelu) tma_store_2d(&tmH, col0 + c0, out_row, smem_u32(bh));
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
         ++groups;

@@ -29,10 +29,11 @@ def test_umma_gemm_matches_fp32_product(M, N, K):
     assert err < 1e-5, err
 
 
-@pytest.mark.parametrize("M,N,K", [(40960, 256, 256), (256, 128, 2048)])
+@pytest.mark.parametrize("M,N,K", [(40960, 256, 256), (256, 128, 2048), (2048, 256, 256), (512, 128, 64)])
 def test_persistent_gemm_epilogues(M, N, K):
     """Bias and bias+GELU through the persistent kernel's TMA-store
-    epilogue (first shape) and the split-K reduction (second), into
+    epilogue (first shape), the split-K reduction (second) and column
+    blocks of 64 columns (third and fourth: few row tiles, short K), into
     matrices whose leading dimension exceeds N."""
     import torch
     from dense_b200.surrogate import EPI_BIAS, EPI_BIAS_GELU, Kernels
