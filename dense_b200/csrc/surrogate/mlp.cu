@@ -430,8 +430,8 @@ int try_persistent(const void* A, int lda, const void* B, int ldb, float* D, int
 
 int gemm_impl(const void* A, int lda, const void* B, int ldb, float* D, int ldd, int M, int N, int K, int epilogue,
               const float* bias, void* H, int ldh, int* err, float* ws, size_t ws_bytes, void* stream) {
-  if ((M % kTileM) || (N % 16) || N < 16 || N > 256 || (K % kChunkK) || (lda % 8) || (ldb % 8) || (ldd % 4) ||
-      (epilogue == kEpiBiasGelu && (ldh % 8 || !H)) || epilogue < kEpiStore || epilogue > kEpiBias ||
+  if (M <= 0 || K <= 0 || (M % kTileM) || (N % 16) || N < 16 || N > 256 || (K % kChunkK) || (lda % 8) ||
+      (ldb % 8) || (ldd % 4) || (epilogue == kEpiBiasGelu && (ldh % 8 || !H)) || epilogue < kEpiStore || epilogue > kEpiBias ||
       (epilogue != kEpiStore && !bias) || !A || !B || !D || !err)
     return 1;
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -40,15 +40,16 @@ def test_surrogate_library_exports_its_entry_points():
 
 def test_surrogate_entry_points_refuse_bad_arguments_on_the_host():
     """Shape and argument checks return 1 before any CUDA call (so they run
-    without a GPU): rows not a multiple of 128, N outside [16, 256], K not a
-    multiple of 64, a bias epilogue without a bias, too many cells for the
+    without a GPU): rows not a positive multiple of 128, N outside [16, 256],
+    K not a positive multiple of 64, a bias epilogue without a bias, too many cells for the
     synchrony kernel, bad encode and score arguments."""
     from dense_b200 import surrogate
     L = ctypes.CDLL(surrogate.build())
     vp, i, i64, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
     L.dense_mlp_gemm_ws.argtypes = [vp, i, vp, i, vp, i, i, i, i, i, vp, vp, i, vp, vp, ctypes.c_size_t, vp]
     p = vp(16)  # never dereferenced: every call below is refused first
-    for M, N, K, epi, bias in ((100, 64, 64, 0, None), (128, 8, 64, 0, None), (128, 512, 64, 0, None),
+    for M, N, K, epi, bias in ((100, 64, 64, 0, None), (0, 64, 64, 0, None), (128, 64, 0, 0, None),
+                               (128, 8, 64, 0, None), (128, 512, 64, 0, None),
                                (128, 64, 96, 0, None), (128, 64, 64, 2, None), (128, 64, 64, 3, p)):
         assert L.dense_mlp_gemm_ws(p, K, p, K, p, N, M, N, K, epi, bias, p, N, p, None, 0, None) == 1
     L.dense_features_synchrony.argtypes = [vp, i64, i64, i, vp, i, vp, vp]
