@@ -171,6 +171,30 @@ def merge_features(*Fs):
     return out
 
 
+def refine(net, P_train, F_train, train, rounds, keep, pool_size, seed, score=None, simulate=None, draw=None):
+    """Refinement rounds (active learning): per round, the current networks
+    rank a fresh pool of `pool_size` candidates (seed + round), the best
+    `keep` (fewer than `pool_size`) are simulated and join the training
+    set, and `train(P, F)` makes new networks from everything.  Returns the final networks, the grown
+    training set and one record per round (pool, simulated, simulation
+    seconds, accepted share, indices kept).  score / simulate / draw
+    default to score_candidates / simulate_features / draw_candidates."""
+    score = score or score_candidates
+    simulate = simulate or simulate_features
+    draw = draw or draw_candidates
+    records = []
+    for r in range(rounds):
+        pool = draw(pool_size, seed + r)
+        top = np.argpartition(-score(net, pool), keep)[:keep]
+        F_new = simulate(pool[top])
+        P_train = np.concatenate([P_train, pool[top]])
+        F_train = merge_features(F_train, F_new)
+        net = train(P_train, F_train)
+        records.append({"pool": pool_size, "simulated": keep, "seconds": F_new["seconds"],
+                        "accepted_fraction_of_simulated": float(accepted(F_new).mean()), "kept": np.sort(top)})
+    return net, P_train, F_train, records
+
+
 def targets(F):
     """Surrogate targets [n][5]: log period, log amplitude, synchrony, the
     oscillation indicator and the acceptance indicator; and their mask

@@ -128,24 +128,22 @@ def main(argv=None):
                             ensemble=a.ensemble)
     res["training_s"] = time.perf_counter() - t1
     res["refine"] = []
-    for r in range(a.refine_rounds if a.refine > 0 else 0):
-        # a round of refinement: the current networks rank a fresh pool, its
+    if a.refine > 0 and a.refine_rounds > 0:
+        # refinement rounds: the current networks rank a fresh pool, its
         # best `refine` candidates are simulated and join the training set
         # (they lie where the search looks), and the networks are trained
         # again on everything; all of it counts in the one-time cost
         t2 = time.perf_counter()
-        pool = S.draw_candidates(a.refine_pool, a.seed + 3 + r)
-        top = np.argpartition(-S.score_candidates(net, pool), a.refine)[:a.refine]
-        F_ref = S.simulate_features(pool[top], log=log, **sim)
-        P_train = np.concatenate([P_train, pool[top]])
-        F_train = S.merge_features(F_train, F_ref)
-        net = S.train_surrogate(P_train, F_train, epochs=a.epochs, batch=2048, seed=a.seed, log=log,
-                                ensemble=a.ensemble)
-        res["refine"].append({"pool": a.refine_pool, "simulated": a.refine, "seconds": F_ref["seconds"],
-                              "accepted_fraction_of_simulated": float(S.accepted(F_ref).mean())})
-        res["training_s"] += time.perf_counter() - t2 - F_ref["seconds"]
+        train = lambda P, F: S.train_surrogate(P, F, epochs=a.epochs, batch=2048, seed=a.seed, log=log,  # noqa
+                                               ensemble=a.ensemble)
+        net, P_train, F_train, rounds = S.refine(net, P_train, F_train, train, a.refine_rounds, a.refine,
+                                                 a.refine_pool, a.seed + 3,
+                                                 simulate=lambda P: S.simulate_features(P, log=log, **sim))
+        sim_s = sum(r["seconds"] for r in rounds)
+        res["refine"] = [{k: v for k, v in r.items() if k != "kept"} for r in rounds]
+        res["training_s"] += time.perf_counter() - t2 - sim_s
         res["data"]["train_sets"] = len(P_train)
-        res["data"]["seconds"] += F_ref["seconds"]
+        res["data"]["seconds"] += sim_s
         res["data"]["accepted_fraction"] = float(S.accepted(F_train).mean())
     res["held_out_error"] = S.feature_errors(net, P_test, F_test)
     res["search_by_horizon"] = {}

@@ -126,3 +126,38 @@ def test_merge_features_concatenates_in_order():
     m = merge_features(a, b)
     assert m["period"].tolist() == [1.0, 2.0, 3.0] and m["status"].tolist() == [0, 1, 2]
     assert m["seconds"] == 2.0 and m["cell_steps"] == 14
+
+
+def test_refinement_rounds_grow_the_training_set_with_the_best_ranked():
+    """Each round ranks a fresh pool, simulates its `keep` best and trains
+    on everything so far (fakes for the network, the scorer and the
+    simulator; the pools differ per round)."""
+    calls = []
+
+    def draw(n, seed):
+        return np.random.Generator(np.random.PCG64(seed)).uniform(size=(n, 3))
+
+    def score(net, P):
+        return P[:, 0] * net        # the "network" is a weight on the first column
+
+    def simulate(P):
+        per = 30.0 + 10.0 * (1.0 - P[:, 0])
+        return {"period": per, "amplitude": np.full(len(P), 60.0), "seconds": 0.5, "cell_steps": len(P)}
+
+    def train(P, F):
+        calls.append((len(P), len(F["period"])))
+        return 1.0 + len(calls)
+
+    P0 = np.zeros((10, 3))
+    F0 = {"period": np.full(10, np.nan), "amplitude": np.full(10, np.nan), "seconds": 1.0, "cell_steps": 10}
+    net, P, F, rec = S.refine(2.0, P0, F0, train, rounds=3, keep=5, pool_size=100, seed=7, score=score,
+                              simulate=simulate, draw=draw)
+    assert calls == [(15, 15), (20, 20), (25, 25)] and net == 4.0
+    assert len(P) == 25 and F["seconds"] == 1.0 + 3 * 0.5 and F["cell_steps"] == 25
+    for r, k in enumerate(rec):
+        pool = draw(100, 7 + r)
+        best = set(np.argsort(-pool[:, 0])[:5].tolist())
+        assert set(k["kept"].tolist()) == best
+        assert set(map(tuple, P[10 + 5 * r:15 + 5 * r])) == set(map(tuple, pool[k["kept"]]))
+    # the best of each pool have period within 30 +- 3 (first column > 0.7) and are accepted
+    assert all(k["accepted_fraction_of_simulated"] > 0.5 for k in rec)
