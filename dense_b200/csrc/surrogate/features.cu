@@ -5,6 +5,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "dense_b200_surrogate.h"
+
 #include <cmath>
 #include <cstdint>
 

@@ -10,6 +10,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "dense_b200_surrogate.h"
+
 #include <cooperative_groups.h>
 
 #include <atomic>

@@ -33,12 +33,14 @@ OUT_PAD = 128   # outputs padded to one UMMA M tile for the weight gradient
 
 
 def build(force=False):
-    srcs = [os.path.join(SRC, f) for f in os.listdir(SRC)]
+    srcs = [os.path.join(SRC, f) for f in os.listdir(SRC)] + [os.path.join(os.path.dirname(HERE), "include",
+                                                                            "dense_b200_surrogate.h")]
     if not force and os.path.exists(LIB) and all(os.path.getmtime(s) <= os.path.getmtime(LIB) for s in srcs):
         return LIB
     os.makedirs(os.path.join(LIB_DIR, "obj"), exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    base = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O3", "-lineinfo"]
+    base = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O3", "-lineinfo",
+            "-I", os.path.join(os.path.dirname(HERE), "include")]
     objs = []
     cmds = []
     for unit in ("mlp", "features"):
